@@ -1,0 +1,173 @@
+"""Seeded synthetic networks with the shapes of the five benchmark workloads.
+
+No dataset is involved: every network, weight and input spike comes from
+``numpy.random.default_rng(seed)``.  Each builder takes a ``scale`` so the same
+construction yields the full-size workload for the benchmark and a reduced copy
+the CPU oracle finishes in seconds for the parity tests.
+
+* :func:`lif_recurrent`     1,000 conductance LIF (800 E / 200 I), p=0.1, 100 Poisson inputs
+                            at 10 Hz, 1 ms delays, Euler dt=0.1 ms.
+* :func:`cerebellar_layer`  AdEx granule layer (in-degree 4 from Poisson mossy fibres at
+                            5-50 Hz) feeding LIF Purkinje cells through plastic (STDP)
+                            synapses; RK4 dt=0.1 ms.
+* :func:`hh_network`        Hodgkin-Huxley neurons, in-degree 100, delays 1-5 ms, one
+                            200 Hz Poisson drive each; BDF order 2 at dt=0.05 ms.
+* :func:`sweep_networks`    many independent LIF networks of uneven size (log-uniform)
+                            with per-network g_leak / E_leak / weight scale; RK2.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .network import Layer, NetworkDescription, poisson_input_times
+
+# LIF parameters for the recurrent workload (the benchmark description fixes
+# E_exc 0, E_inh -80, E_L -65, v_thr -50, tau_ref 1 ms, tau_AMPA 0.5 ms,
+# tau_GABA 10 ms and leaves C_m / g_L to the builder; these put the network in
+# the 5-30 Hz range).
+LIF_C1 = dict(e_exc=0.0, e_inh=-80.0, e_leak=-65.0, v_thr=-50.0, c_m=2.0, tau_exc=0.5,
+              tau_inh=10.0, tau_ref=1.0, g_leak=0.2, tau_nmda=20.0)
+
+
+def lif_recurrent(seed: int = 1, n: int = 1000, n_inputs: int = 100, p: float = 0.1,
+                  rate_hz: float = 10.0, t_end: float = 1.0, dt: float = 1e-4,
+                  integrator: str = "Euler", model: str = "LIFTimeDrivenModel",
+                  params: dict | None = None, w_exc_max: float = 0.5, w_inh_max: float = 2.0,
+                  delay: float = 1e-3, bdf_order: int = 2):
+    """Recurrent E/I LIF network driven by Poisson inputs.
+
+    Neurons 0..n_inputs-1 are ``InputSpikeNeuronModel`` (their spikes come from the
+    returned input list); n_inputs.. are one LIF layer whose first 80% project
+    excitatory (type 0) and last 20% inhibitory (type 1) synapses.
+    Returns (NetworkDescription, input_times, input_cells).
+    """
+    rng = np.random.default_rng(seed)
+    net = NetworkDescription()
+    inp = net.add_layer(Layer(n_inputs, "InputSpikeNeuronModel", output=0))
+    lif = net.add_layer(Layer(n, model, dict(params or LIF_C1), integrator=integrator, dt=dt,
+                              bdf_order=bdf_order, name="lif"))
+    n_exc = int(round(0.8 * n))
+    sources = np.arange(n_inputs + n)
+    mask = rng.random((len(sources), n)) < p
+    s_idx, t_idx = np.nonzero(mask)
+    src = sources[s_idx]
+    tgt = lif.start + t_idx
+    inh = src >= lif.start + n_exc
+    stype = np.where(inh, 1, 0).astype(np.int32)
+    wmax = np.where(inh, w_inh_max, w_exc_max).astype(np.float32)
+    w = (rng.random(len(src)) * wmax).astype(np.float32)
+    net.add_synapses(src, tgt, delay, stype, w, wmax, -1)
+    times, cells = poisson_input_times(rng, n_inputs, rate_hz, t_end, dt)
+    return net, times, cells + inp.start
+
+
+def cerebellar_layer(seed: int = 1, n_granule: int = 250_000, n_mossy: int = 5_000,
+                     n_purkinje: int = 200, pf_per_purkinje: int = 50_000,
+                     t_end: float = 1.0, dt: float = 1e-4, integrator: str = "RK4",
+                     w_mf: float = 4.0, w_pf: float = 0.05, w_pf_max: float = 0.1,
+                     stdp=(1e-3, 0.020, 1.05e-3, 0.020), delay: float = 1e-3,
+                     granule_params: dict | None = None, purkinje_params: dict | None = None):
+    """Granule (AdEx) layer with in-degree 4 from Poisson mossy fibres at U[5,50] Hz,
+    and Purkinje (LIF) cells each receiving ``pf_per_purkinje`` granule synapses
+    drawn without replacement, all plastic under additive STDP.
+    Returns (NetworkDescription, input_times, input_cells)."""
+    rng = np.random.default_rng(seed)
+    net = NetworkDescription()
+    mf = net.add_layer(Layer(n_mossy, "InputSpikeNeuronModel", output=0))
+    grc = net.add_layer(Layer(n_granule, "AdExTimeDrivenModel", dict(granule_params or {}),
+                              integrator=integrator, dt=dt, name="granule"))
+    pc = net.add_layer(Layer(n_purkinje, "LIFTimeDrivenModel",
+                             dict(purkinje_params or dict(c_m=100.0, g_leak=5.0, tau_exc=2.0)),
+                             integrator=integrator, dt=dt, name="purkinje"))
+    net.rules.append(("STDP", list(stdp)))
+    # mossy fibre -> granule: in-degree exactly 4
+    src = rng.integers(0, n_mossy, size=(n_granule, 4)) + mf.start
+    tgt = np.repeat(np.arange(n_granule) + grc.start, 4)
+    net.add_synapses(src.ravel(), tgt, delay, 0, w_mf, w_mf, -1)
+    # granule -> Purkinje: pf_per_purkinje distinct granules per Purkinje cell
+    k = min(pf_per_purkinje, n_granule)
+    srcs = np.empty((n_purkinje, k), np.int64)
+    for j in range(n_purkinje):
+        srcs[j] = rng.choice(n_granule, size=k, replace=False)
+    srcs += grc.start
+    tgts = np.repeat(np.arange(n_purkinje) + pc.start, k)
+    wpf = (rng.random(n_purkinje * k) * 2 * w_pf).astype(np.float32)
+    net.add_synapses(srcs.ravel(), tgts, delay, 0, np.minimum(wpf, w_pf_max), w_pf_max, 0)
+    rates = rng.uniform(5.0, 50.0, n_mossy)
+    times, cells = poisson_input_times(rng, n_mossy, rates, t_end, dt)
+    return net, times, cells + mf.start
+
+
+def hh_network(seed: int = 1, n: int = 100_000, indeg: int = 100, t_end: float = 0.5,
+               dt: float = 5e-5, drive_hz: float = 200.0, w_exc: float = 3.0,
+               w_inh: float = 12.0, w_drive: float = 30.0, bdf_order: int = 2,
+               integrator: str = "BDF", params: dict | None = None):
+    """Hodgkin-Huxley network: fixed in-degree from uniformly random sources (80% of
+    sources excitatory), integer delays of 1-5 ms, one Poisson drive per neuron at
+    ``drive_hz`` through a 1 ms excitatory synapse.
+    Returns (NetworkDescription, input_times, input_cells)."""
+    rng = np.random.default_rng(seed)
+    net = NetworkDescription()
+    drv = net.add_layer(Layer(n, "InputSpikeNeuronModel", output=0))
+    hh = net.add_layer(Layer(n, "HHTimeDrivenModel", dict(params or {}), integrator=integrator,
+                             dt=dt, bdf_order=bdf_order, name="hh"))
+    n_exc = int(round(0.8 * n))
+    src = rng.integers(0, n, size=(n, indeg))
+    tgt = np.repeat(np.arange(n), indeg)
+    src = src.ravel()
+    inh = src >= n_exc
+    delay = rng.integers(1, 6, size=len(src)).astype(np.float32) * np.float32(1e-3)
+    net.add_synapses(src + hh.start, tgt + hh.start, delay, inh.astype(np.int32),
+                     np.where(inh, w_inh, w_exc), np.where(inh, w_inh, w_exc), -1)
+    net.add_synapses(np.arange(n) + drv.start, np.arange(n) + hh.start, 1e-3, 0, w_drive,
+                     w_drive, -1)
+    times, cells = poisson_input_times(rng, n, drive_hz, t_end, dt)
+    return net, times, cells + drv.start
+
+
+def sweep_sizes(seed: int = 1, n_networks: int = 4096, n_min: int = 500, n_max: int = 5000):
+    """Network sizes log-uniform in [n_min, n_max]."""
+    rng = np.random.default_rng(seed)
+    return np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_networks)).astype(np.int64)
+
+
+# Per-model synaptic weight ranges that give moderate firing in parity_network.
+_PARITY_W = {
+    "LIFTimeDrivenModel": dict(w_in=0.5, w_exc=0.5, w_inh=2.0),
+    "AdExTimeDrivenModel": dict(w_in=6.0, w_exc=2.0, w_inh=4.0),
+    "HHTimeDrivenModel": dict(w_in=40.0, w_exc=10.0, w_inh=20.0),
+}
+
+
+def parity_network(model: str = "LIFTimeDrivenModel", integrator: str = "Euler", seed: int = 1,
+                   n: int = 200, n_inputs: int = 40, p: float = 0.1, rate_hz: float = 20.0,
+                   t_end: float = 0.2, dt: float = 1e-4, bdf_order: int = 2, stdp: bool = False,
+                   delays=(1e-3,), params: dict | None = None, weights: dict | None = None):
+    """Small recurrent E/I network of one model, for step-level parity against the
+    reference: Poisson inputs, p-connectivity, one or several delays, optional STDP on
+    the excitatory recurrent synapses.  Returns (NetworkDescription, in_times, in_cells)."""
+    rng = np.random.default_rng(seed)
+    w = dict(_PARITY_W[model.replace("_GPU", "")])
+    w.update(weights or {})
+    net = NetworkDescription()
+    inp = net.add_layer(Layer(n_inputs, "InputSpikeNeuronModel", output=0))
+    pop = net.add_layer(Layer(n, model, dict(params or {}), integrator=integrator, dt=dt,
+                              bdf_order=bdf_order, name="pop"))
+    if stdp:
+        net.rules.append(("STDP", [0.05 * w["w_exc"], 0.020, 0.0525 * w["w_exc"], 0.020]))
+    n_exc = int(round(0.8 * n))
+    # input -> population (dense-ish so every neuron is driven)
+    m_in = rng.random((n_inputs, n)) < max(p, 0.25)
+    s, t = np.nonzero(m_in)
+    net.add_synapses(s + inp.start, t + pop.start, delays[0], 0,
+                     (rng.random(len(s)) * w["w_in"]).astype(np.float32), w["w_in"], -1)
+    mr = rng.random((n, n)) < p
+    s, t = np.nonzero(mr)
+    inh = s >= n_exc
+    d = np.asarray(delays, np.float32)[rng.integers(0, len(delays), len(s))]
+    wmax = np.where(inh, w["w_inh"], w["w_exc"]).astype(np.float32)
+    ww = (rng.random(len(s)) * wmax).astype(np.float32)
+    rule = np.where(inh | (not stdp), -1, 0).astype(np.int32)
+    net.add_synapses(s + pop.start, t + pop.start, d, inh.astype(np.int32), ww, wmax, rule)
+    times, cells = poisson_input_times(rng, n_inputs, rate_hz, t_end, dt)
+    return net, times, cells + inp.start
