@@ -1,0 +1,90 @@
+"""ctypes binding of libedlut_b200.so (the C ABI declared in include/edlut_b200.h).
+
+The library is built in-tree (``edlut_b200/_lib/libedlut_b200.so``) by
+:func:`edlut_b200.build.build`.  Loading fails loudly when it is missing: there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libedlut_b200.so")
+
+EB_OK = 0
+ERRORS = {-1: "EB_ERR_ARG", -2: "EB_ERR_CUDA", -3: "EB_ERR_STATE", -4: "EB_ERR_OVERFLOW",
+          -5: "EB_ERR_PARSE", -6: "EB_ERR_UNSUPPORTED", -7: "EB_ERR_NOMEM", -8: "EB_ERR_NUMERIC"}
+KINDS = {"InputSpikeNeuronModel": 0, "LIFTimeDrivenModel": 1, "AdExTimeDrivenModel": 2,
+         "HHTimeDrivenModel": 3}
+INTEGRATORS = {"Euler": 0, "RK2": 1, "RK4": 2, "BDF": 3}
+
+c_i64p = ctypes.POINTER(ctypes.c_int64)
+c_f32p = ctypes.POINTER(ctypes.c_float)
+c_i32p = ctypes.POINTER(ctypes.c_int32)
+c_f64p = ctypes.POINTER(ctypes.c_double)
+
+# (name, restype, argtypes) of every exported entry point
+SIGNATURES = [
+    ("eb_last_error", ctypes.c_char_p, []),
+    ("eb_version", ctypes.c_char_p, []),
+    ("eb_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("eb_ctx_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("eb_add_population", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_float, c_f32p, ctypes.c_int, c_i64p]),
+    ("eb_add_stdp_rule", ctypes.c_int, [ctypes.c_void_p, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                         ctypes.c_float, ctypes.POINTER(ctypes.c_int)]),
+    ("eb_set_connectivity", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_i64p, c_i64p, c_f32p, c_i32p,
+                                            c_f32p, c_f32p, c_i32p]),
+    ("eb_set_bucket_limit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
+    ("eb_finalize", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
+    ("eb_load_network_files", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p]),
+    ("eb_inject_spikes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_f32p, c_i64p]),
+    ("eb_load_input_file", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
+    ("eb_run", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("eb_run_async", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("eb_sync", ctypes.c_int, [ctypes.c_void_p]),
+    ("eb_set_graph_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("eb_set_record_capacity", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("eb_get_spikes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_i64p, c_i64p, c_i64p]),
+    ("eb_step_time", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_f64p]),
+    ("eb_get_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, c_f32p]),
+    ("eb_set_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, c_f32p]),
+    ("eb_set_trace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64]),
+    ("eb_get_trace", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
+    ("eb_get_weights", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
+    ("eb_set_weights", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
+    ("eb_get_counters", ctypes.c_int, [ctypes.c_void_p, c_i64p, c_i64p, c_i64p]),
+    ("eb_device_bytes", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
+    ("eb_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("eb_restore", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+]
+
+_lib = None
+
+
+class EdlutError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "EB_ERR"), code, msg))
+        self.code = code
+
+
+def load():
+    """Load libedlut_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("edlut_b200 CUDA library not built: %s is missing "
+                               "(run __graft_entry__.build() or python -m edlut_b200.build)" % LIB_PATH)
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != EB_OK:
+        raise EdlutError(rc, load().eb_last_error().decode())

@@ -1,0 +1,363 @@
+// Device-side neuron models and integrators of the time-driven hot path.
+//
+// One thread (or one warp lane) owns one neuron; the integrator stages live in
+// registers.  The arithmetic follows the reference CPU models operation by
+// operation (same float/double promotions, same lookup tables computed on the
+// host, no FMA contraction: the library is compiled with --fmad=false), so a
+// neuron update here produces the same float32 bits as the reference:
+//   LIF  src/neuron_model/LIFTimeDrivenModel.cpp:160-242
+//   AdEx src/neuron_model/AdExTimeDrivenModel.cpp:157-235
+//   HH   src/neuron_model/HHTimeDrivenModel.cpp:188-276, rate table HHTimeDrivenModel.h:372-441
+//   Euler include/integration_method/Euler.h:123-146, RK2 RK2.h:133-165,
+//   RK4 RK4.h:167-231, BDFn BDFn.h:288-420 (Jacobian :704-724, inverse :735-797).
+#pragma once
+#include <cstdint>
+#include "eb_types.h"
+
+namespace eb {
+
+constexpr float kExptMin = -20.0f;
+constexpr float kExptMax = 20.0f;
+constexpr float kHHMinV = -90.0f;
+
+// ExponentialTable::GetResult (include/simulation/ExponentialTable.h:92-103).
+__device__ __forceinline__ float expt(const PopDev &P, float v) {
+    if (v >= kExptMin && v <= kExptMax) {
+        int pos = (int)((v - kExptMin) * P.expt_aux);
+        return __ldg(P.exp_table + pos);
+    }
+    if (v > kExptMax) return (float)exp((double)v);
+    return 0.0f;
+}
+
+__device__ __forceinline__ float nmda_inf(const PopDev &P, float v, float e_inh) {
+    int pos = (int)((v - e_inh) * P.nmda_aux);
+    if (pos < 0) pos = 0; else if (pos > kNmdaTable - 1) pos = kNmdaTable - 1;
+    return __ldg(P.nmda_table + pos);
+}
+
+// -------------------------------------------------------------------- LIF --
+// x = {V, gE, gI, gNMDA}; refr = updates since the last spike (-1: never spiked,
+// LastSpikeTime >= 100 s).  LastSpikeTime = refr * dt exactly, because every
+// partial sum of the reference's double accumulation is exact.
+__device__ __forceinline__ void lif_deriv(const PopDev &P, const float *x, float *dx, int refr) {
+    const float *p = P.p;  // e_exc e_inh e_leak v_thr c_m tau_exc tau_inh tau_ref g_leak tau_nmda
+    float current = 0.0f;
+    if (P.en & 1) current += x[1] * (p[0] - x[0]);
+    if (P.en & 2) current += x[2] * (p[1] - x[0]);
+    if (P.en & 4) current += x[3] * nmda_inf(P, x[0], p[1]) * (p[0] - x[0]);
+    float full = (current + p[8] * (p[2] - x[0])) * P.inv_c_m;
+    if (refr < 0) { dx[0] = full; return; }
+    double l = ((double)refr * (double)P.dt_s) * 1000.0;
+    if (l > (double)p[7]) {
+        dx[0] = full;
+    } else if (l + (double)P.dt_ms > (double)p[7]) {
+        float fraction = (float)((l + (double)P.dt_ms - (double)p[7]) / (double)P.dt_ms);
+        dx[0] = fraction * full;
+    } else {
+        dx[0] = 0.0f;
+    }
+}
+
+// ------------------------------------------------------------------- AdEx --
+// p = a b thr_slo_fac v_thr tau_w e_exc e_inh e_reset e_leak g_leak c_m tau_exc tau_inh tau_nmda
+// x = {V, w, gE, gI, gNMDA}
+__device__ __forceinline__ void adex_deriv(const PopDev &P, const float *x, float *dx) {
+    const float *p = P.p;
+    const float a = p[0], slope = p[2], vthr = p[3], eexc = p[5], einh = p[6], eleak = p[8], gl = p[9];
+    if (x[0] <= vthr + 6 * slope) {
+        float current = 0.0f;
+        if (P.en & 1) current += x[2] * (eexc - x[0]);
+        if (P.en & 2) current += x[3] * (einh - x[0]);
+        if (P.en & 4) current += x[4] * nmda_inf(P, x[0], einh) * (eexc - x[0]);
+        dx[0] = (gl * (eleak - x[0]) + gl * slope * expt(P, (x[0] - vthr) * P.inv_slope) - x[1] + current) * P.inv_c_m;
+        dx[1] = (a * (x[0] - eleak) - x[1]) * P.inv_tau_w;
+    } else if (x[0] <= 0.0f) {
+        const float Vm = vthr + 6 * slope;
+        float current = 0.0f;
+        if (P.en & 1) current += x[2] * (eexc - Vm);
+        if (P.en & 2) current += x[3] * (einh - Vm);
+        if (P.en & 4) current += x[4] * nmda_inf(P, Vm, einh) * (eexc - Vm);
+        dx[0] = (gl * (eleak - Vm) + gl * slope * expt(P, (Vm - vthr) * P.inv_slope) - x[1] + current) * P.inv_c_m;
+        dx[1] = (a * (x[0] - eleak) - x[1]) * P.inv_tau_w;
+    } else {
+        dx[0] = 0.0f;
+        dx[1] = 0.0f;
+    }
+}
+
+// --------------------------------------------------------------------- HH --
+// p = e_exc e_inh e_leak g_leak c_m v_thr tau_exc tau_inh tau_nmda g_na g_kd e_na e_k
+// x = {V, m, h, n, gE, gI, gNMDA}.  The clamps write the state passed in, as the
+// reference does (HHTimeDrivenModel.cpp:197-222).
+__device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
+    const float *p = P.p;
+    const float eexc = p[0], einh = p[1], eleak = p[2], gl = p[3], gna = p[9], gkd = p[10], ena = p[11], ek = p[12];
+    if (x[0] < ek) x[0] = ek;
+    if (x[0] > ena - 1.0f) x[0] = ena - 1.0f;
+    if (x[1] < 0) x[1] = 0.0f;
+    if (x[1] > 1) x[1] = 1.0f;
+    if (x[2] < 0) x[2] = 0.0f;
+    if (x[2] > 1) x[2] = 1.0f;
+    if (x[3] < 0) x[3] = 0.0f;
+    if ((double)x[3] > 0.72) x[3] = 0.72f;
+    const float V = x[0], m = x[1], h = x[2], n = x[3];
+    int pos = (int)((V - kHHMinV) * P.hh_aux);
+    if (pos < 0) pos = 0; else if (pos > kHHTable - 1) pos = kHHTable - 1;
+    const float *r = P.hh_table + (size_t)pos * 6;
+    const float am = __ldg(r + 0), bm = __ldg(r + 1), ah = __ldg(r + 2), bh = __ldg(r + 3), an = __ldg(r + 4), bn = __ldg(r + 5);
+    float current = 0.0f;
+    if (P.en & 1) current += x[4] * (eexc - x[0]);
+    if (P.en & 2) current += x[5] * (einh - x[0]);
+    if (P.en & 4) current += x[6] * nmda_inf(P, x[0], einh) * (eexc - x[0]);
+    dx[0] = (current + gl * (eleak - V) + gna * m * m * m * h * (ena - V) + gkd * n * n * n * n * (ek - V)) * P.inv_c_m;
+    dx[1] = (am * (1.0f - m) - bm * m);
+    dx[2] = (ah * (1.0f - h) - bh * h);
+    dx[3] = (an * (1.0f - n) - bn * n);
+}
+
+template <int KIND> struct Model;
+template <> struct Model<KIND_LIF> {
+    static constexpr int ND = 1, NV = 4;
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, int refr) { lif_deriv(P, x, dx, refr); }
+};
+template <> struct Model<KIND_ADEX> {
+    static constexpr int ND = 2, NV = 5;
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, int) { adex_deriv(P, x, dx); }
+};
+template <> struct Model<KIND_HH> {
+    static constexpr int ND = 4, NV = 7;
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, int) { hh_deriv(P, x, dx); }
+};
+
+// EvaluateTimeDependentEquation: g <- 0 below 1e-9, else g * factor (enabled types only).
+template <int ND>
+__device__ __forceinline__ void decay(const PopDev &P, float *x) {
+    const float limit = 1e-9;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        if (!(P.en & (1 << c))) continue;
+        if (x[ND + c] < limit) x[ND + c] = 0.0f;
+        else x[ND + c] *= P.decay[c];
+    }
+}
+
+// Gauss-Jordan inverse with the reference's zero-pivot row swap (BDFn.h:735-797).
+template <int N>
+__device__ __forceinline__ bool invermat(const float *a, float *ainv) {
+    if constexpr (N == 1) {
+        ainv[0] = 1.0f / a[0];
+        return true;
+    }
+    float la[N * N], li[N * N];
+#pragma unroll
+    for (int i = 0; i < N * N; ++i) { la[i] = a[i]; li[i] = 0.0f; }
+#pragma unroll
+    for (int i = 0; i < N; ++i) li[i * N + i] = 1.0f;
+#pragma unroll
+    for (int s = 0; s < N; ++s) {
+        float el = la[s * N + s];
+        if (el == 0) {
+            bool found = false;
+#pragma unroll
+            for (int r = s + 1; r < N; ++r) {
+                if (found) break;
+                el = la[r * N + s];
+                if (el != 0) {
+#pragma unroll
+                    for (int c = 0; c < N; ++c) {
+                        float v = la[r * N + c]; la[r * N + c] = la[s * N + c]; la[s * N + c] = v;
+                        v = li[r * N + c]; li[r * N + c] = li[s * N + c]; li[s * N + c] = v;
+                    }
+                    found = true;
+                } else if (r == N - 1) {
+                    return false;
+                }
+            }
+        }
+        const float inv = 1.0f / el;
+#pragma unroll
+        for (int c = 0; c < N; ++c) { la[s * N + c] *= inv; li[s * N + c] *= inv; }
+#pragma unroll
+        for (int r = 0; r < N; ++r) {
+            if (r == s) continue;
+            const float coef = -la[r * N + s];
+#pragma unroll
+            for (int c = 0; c < N; ++c) {
+                la[r * N + c] += la[s * N + c] * coef;
+                li[r * N + c] += li[s * N + c] * coef;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < N * N; ++i) ainv[i] = li[i];
+    return true;
+}
+
+// Per-neuron BDF history, SoA in global memory: D[q][v][n], P[q][v][n].
+struct BdfRef {
+    float *D, *Pv;
+    int64_t stride;  // population size
+    int64_t i;
+    __device__ float &d(int q, int v, int nd) const { return D[((int64_t)q * nd + v) * stride + i]; }
+    __device__ float &pv(int q, int v, int nd) const { return Pv[((int64_t)q * nd + v) * stride + i]; }
+};
+
+// One integration step of one neuron.  x holds all NV state variables.  Returns
+// false only if the BDF Newton matrix was singular.
+template <int KIND, int INTEG>
+__device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, int &bdf_state, const BdfRef &H) {
+    using M = Model<KIND>;
+    constexpr int ND = M::ND, NV = M::NV;
+    const float dt = P.dt_ms;
+    float k1[NV], k2[NV], k3[NV], k4[NV], aux[NV];
+    if (INTEG == INTEG_EULER) {
+        M::deriv(P, x, k1, refr);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) x[j] += dt * k1[j];
+        decay<ND>(P, x);
+    } else if (INTEG == INTEG_RK2) {
+        M::deriv(P, x, k1, refr);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) x[j] += k1[j] * dt;
+        decay<ND>(P, x);
+        M::deriv(P, x, k2, refr);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) x[j] += (-k1[j] + k2[j]) * dt * 0.5f;
+    } else if (INTEG == INTEG_RK4) {
+        const float h05 = dt * 0.5f;
+        const float h016 = dt * 0.166666666667f;
+        M::deriv(P, x, k1, refr);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) aux[j] = x[j] + k1[j] * h05;
+#pragma unroll
+        for (int j = ND; j < NV; ++j) aux[j] = x[j];
+        decay<ND>(P, aux);
+        M::deriv(P, aux, k2, refr);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) aux[j] = x[j] + k2[j] * h05;
+        M::deriv(P, aux, k3, refr);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) aux[j] = x[j] + k3[j] * dt;
+        decay<ND>(P, aux);
+        M::deriv(P, aux, k4, refr);
+#pragma unroll
+        for (int j = 0; j < ND; ++j) x[j] += (k1[j] + 2.0f * (k2[j] + k3[j]) + k4[j]) * h016;
+#pragma unroll
+        for (int j = ND; j < NV; ++j) x[j] = aux[j];
+    } else {  // BDFn
+        int st = bdf_state;
+        float pr[NV], p1[ND], c[ND], jac[ND * ND], J[ND * ND], iJ[ND * ND];
+        if (st == 0) {
+            M::deriv(P, x, aux, refr);
+#pragma unroll
+            for (int j = 0; j < ND; ++j) pr[j] = x[j] + dt * aux[j];
+        } else {
+#pragma unroll
+            for (int j = 0; j < ND; ++j) {
+                pr[j] = x[j];
+                for (int q = 0; q < st; ++q) pr[j] += H.d(q, j, ND);
+            }
+        }
+#pragma unroll
+        for (int j = ND; j < NV; ++j) pr[j] = x[j];
+        decay<ND>(P, pr);
+        const float *co = P.bdf_coef[st];
+        float hist[6][ND];
+        for (int q = 1; q < st; ++q)
+#pragma unroll
+            for (int j = 0; j < ND; ++j) hist[q - 1][j] = H.pv(q - 1, j, ND);
+        float epsi = 1.0f;
+        int k = 0;
+        const float eps_j = dt * 0.1f;
+        const float inv_eps = 1.0f / eps_j;
+        while (epsi > 1e-6 && k < 10) {
+            M::deriv(P, pr, aux, refr);
+#pragma unroll
+            for (int j = 0; j < ND; ++j) {
+                c[j] = co[0] * dt * aux[j] + co[1] * x[j];
+                for (int q = 1; q < st; ++q) c[j] += co[q + 1] * hist[q - 1][j];
+            }
+            // Jacobian: one-sided difference at eps = 0.1 dt (BDFn.h:704-724)
+            {
+                float tmp[NV], pos[NV], neg[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) tmp[v] = pr[v];
+                M::deriv(P, tmp, pos, refr);
+#pragma unroll
+                for (int j = 0; j < ND; ++j) {
+#pragma unroll
+                    for (int v = 0; v < NV; ++v) tmp[v] = pr[v];
+                    tmp[j] -= eps_j;
+                    M::deriv(P, tmp, neg, refr);
+#pragma unroll
+                    for (int z = 0; z < ND; ++z) jac[z * ND + j] = (pos[z] - neg[z]) * inv_eps;
+                }
+            }
+#pragma unroll
+            for (int z = 0; z < ND; ++z)
+#pragma unroll
+                for (int t = 0; t < ND; ++t) {
+                    J[z * ND + t] = co[0] * dt * jac[z * ND + t];
+                    if (z == t) J[z * ND + t] -= 1;
+                }
+            if (!invermat<ND>(J, iJ)) return false;
+#pragma unroll
+            for (int z = 0; z < ND; ++z) {
+                float a = 0.0f;
+#pragma unroll
+                for (int t = 0; t < ND; ++t) a += iJ[z * ND + t] * (pr[t] - c[t]);
+                p1[z] = a + pr[z];
+            }
+            float mx = 0.0f;
+#pragma unroll
+            for (int z = 0; z < ND; ++z) {
+                float d = fabsf(p1[z] - pr[z]);
+                if (d > mx) mx = d;
+            }
+#pragma unroll
+            for (int z = 0; z < ND; ++z) pr[z] = p1[z];
+            epsi = mx;
+            k++;
+        }
+        if (st < P.bdf_order) st++;
+        bdf_state = st;
+#pragma unroll
+        for (int j = 0; j < ND; ++j) {
+            float dq[7];
+            for (int q = 0; q < st; ++q) dq[q] = H.d(q, j, ND);
+            for (int q = st - 1; q > 0; --q) dq[q] = -dq[q - 1];
+            dq[0] = pr[j] - x[j];
+            for (int q = 1; q < st; ++q) dq[q] += dq[q - 1];
+            for (int q = 0; q < st; ++q) H.d(q, j, ND) = dq[q];
+        }
+        if (st > 1) {
+            for (int q = st - 2; q > 0; --q)
+#pragma unroll
+                for (int j = 0; j < ND; ++j) H.pv(q, j, ND) = hist[q - 1][j];
+#pragma unroll
+            for (int j = 0; j < ND; ++j) H.pv(0, j, ND) = x[j];
+        }
+#pragma unroll
+        for (int j = 0; j < ND; ++j) x[j] = pr[j];
+        decay<ND>(P, x);
+    }
+    return true;
+}
+
+// EvaluateSpikeCondition of the three models.  Returns true on a spike; sets
+// reset when the model restarts its integrator history (LIF, AdEx; not HH).
+template <int KIND>
+__device__ __forceinline__ bool spike_condition(const PopDev &P, float *x, float prevV, bool &reset) {
+    reset = false;
+    if (KIND == KIND_LIF) {
+        if (x[0] > P.p[3]) { x[0] = P.p[2]; reset = true; return true; }
+    } else if (KIND == KIND_ADEX) {
+        if (x[0] > 0.0f) { x[0] = P.p[7]; x[1] += P.p[1]; reset = true; return true; }
+    } else {
+        if (x[0] > -30.0f && prevV < -30.0f) return true;
+    }
+    return false;
+}
+
+}  // namespace eb

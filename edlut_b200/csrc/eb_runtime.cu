@@ -1,0 +1,869 @@
+// Host runtime of the device-resident network: construction of the device
+// tables, the K-step run loop (CUDA graphs), I/O, and the C ABI of
+// include/edlut_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "edlut_b200.h"
+#include "eb_kernels.h"
+#include "eb_runtime.h"
+#include "eb_tables.h"
+
+using namespace eb;
+
+static thread_local std::string g_err;
+
+void eb::set_error(const char *fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return EB_ERR_CUDA;                                                               \
+        }                                                                                     \
+    } while (0)
+
+namespace {
+
+int model_nv(int kind) { return kind == KIND_LIF ? 4 : kind == KIND_ADEX ? 5 : kind == KIND_HH ? 7 : 0; }
+int model_nd(int kind) { return kind == KIND_LIF ? 1 : kind == KIND_ADEX ? 2 : kind == KIND_HH ? 4 : 0; }
+int model_nparams(int kind) { return kind == KIND_LIF ? 10 : kind == KIND_ADEX ? 14 : kind == KIND_HH ? 13 : 0; }
+
+}  // namespace
+
+// ------------------------------------------------------------- allocation --
+int eb_ctx::dalloc(void **p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        set_error("cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+        return EB_ERR_NOMEM;
+    }
+    allocs.push_back(*p);
+    dev_bytes += (int64_t)bytes;
+    return EB_OK;
+}
+
+void eb_ctx::dfree_all() {
+    for (void *p : allocs) cudaFree(p);
+    allocs.clear();
+    dev_bytes = 0;
+}
+
+template <class T>
+static int upload(eb_ctx *c, T **dptr, const std::vector<T> &h) {
+    int rc = c->dalloc((void **)dptr, h.size() * sizeof(T));
+    if (rc) return rc;
+    if (!h.empty()) CK(cudaMemcpyAsync(*dptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    return EB_OK;
+}
+
+// ----------------------------------------------------------- construction --
+int eb_ctx::add_population(int kind, int64_t n, int integ, int bdf_order, float dt, const float *params,
+                           int n_params, int64_t *out_first) {
+    if (finalized) { set_error("eb_add_population after eb_finalize"); return EB_ERR_STATE; }
+    if (n <= 0 || kind < KIND_INPUT || kind > KIND_HH) { set_error("bad population kind/size"); return EB_ERR_ARG; }
+    HostPop p;
+    p.kind = kind;
+    p.n = n;
+    p.first = n_neurons;
+    if (kind != KIND_INPUT) {
+        if (integ < INTEG_EULER || integ > INTEG_BDF) { set_error("unsupported integrator %d", integ); return EB_ERR_UNSUPPORTED; }
+        if (integ == INTEG_BDF && (bdf_order < 1 || bdf_order > 6)) { set_error("BDF order must be 1..6"); return EB_ERR_ARG; }
+        if (!(dt > 0.0f)) { set_error("integration step must be > 0"); return EB_ERR_ARG; }
+        if (n_params != model_nparams(kind) || !params) {
+            set_error("model kind %d takes %d parameters, got %d", kind, model_nparams(kind), n_params);
+            return EB_ERR_ARG;
+        }
+        if (kind == KIND_LIF && params[7] >= 1.0e5f) { set_error("tau_ref must be < 1e5 ms"); return EB_ERR_UNSUPPORTED; }
+        p.params.assign(params, params + n_params);
+        p.integ = integ;
+        p.bdf_order = integ == INTEG_BDF ? bdf_order : 0;
+        p.dt = dt;
+    }
+    if (out_first) *out_first = p.first;
+    n_neurons += n;
+    pops.push_back(p);
+    return EB_OK;
+}
+
+int eb_ctx::finalize(int64_t *out_sorted_perm) {
+    if (finalized) { set_error("eb_finalize called twice"); return EB_ERR_STATE; }
+    if (n_neurons <= 0) { set_error("no populations"); return EB_ERR_STATE; }
+    const int64_t m = (int64_t)src.size();
+    // step size shared by all model populations
+    dt_f = 0.0f;
+    for (auto &p : pops)
+        if (p.kind != KIND_INPUT) {
+            if (dt_f == 0.0f) dt_f = p.dt;
+            else if (p.dt != dt_f) { set_error("all model populations must share one integration step"); return EB_ERR_UNSUPPORTED; }
+        }
+    if (dt_f == 0.0f) dt_f = 1e-4f;
+    dt_s = (double)dt_f;
+    pop_of.assign(n_neurons, 0);
+    for (size_t q = 0; q < pops.size(); ++q)
+        for (int64_t i = 0; i < pops[q].n; ++i) pop_of[pops[q].first + i] = (int)q;
+    // validate synapses, enable conductance types per target population
+    std::vector<int64_t> units(m);
+    int64_t max_units = 1;
+    for (int64_t k = 0; k < m; ++k) {
+        if (src[k] < 0 || src[k] >= n_neurons || tgt[k] < 0 || tgt[k] >= n_neurons) {
+            set_error("synapse %lld: neuron index out of range", (long long)k);
+            return EB_ERR_ARG;
+        }
+        HostPop &tp = pops[pop_of[tgt[k]]];
+        if (tp.kind == KIND_INPUT) { set_error("synapse %lld targets an input neuron", (long long)k); return EB_ERR_UNSUPPORTED; }
+        if (stype[k] < 0 || stype[k] > 2) {
+            set_error("synapse %lld: type %d (only 0 AMPA, 1 GABA, 2 NMDA spike synapses)", (long long)k, stype[k]);
+            return EB_ERR_UNSUPPORTED;
+        }
+        if (rule[k] >= (int32_t)rules.size()) { set_error("synapse %lld: learning rule %d undefined", (long long)k, rule[k]); return EB_ERR_ARG; }
+        tp.en |= 1 << stype[k];
+        units[k] = delay_units(delay[k]);
+        if (units[k] > 65535) { set_error("delay above 6.5535 s"); return EB_ERR_UNSUPPORTED; }
+        max_units = std::max(max_units, units[k]);
+    }
+    // reference synapse order: (source, delay, target), ties by original index
+    std::vector<int64_t> ord(m);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) {
+        if (src[a] != src[b]) return src[a] < src[b];
+        if (units[a] != units[b]) return units[a] < units[b];
+        return tgt[a] < tgt[b];
+    });
+    if (out_sorted_perm) std::copy(ord.begin(), ord.end(), out_sorted_perm);
+    spos_of.assign(m, 0);
+    for (int64_t s = 0; s < m; ++s) spos_of[ord[s]] = s;
+    std::vector<int64_t> out_ptr(n_neurons + 1, 0);
+    for (int64_t k = 0; k < m; ++k) out_ptr[src[k] + 1]++;
+    for (int64_t i = 0; i < n_neurons; ++i) out_ptr[i + 1] += out_ptr[i];
+    // target-major order: per target, plastic first, then reference order
+    std::vector<int64_t> in_ptr(n_neurons + 1, 0), plastic_end(n_neurons, 0);
+    std::vector<int64_t> indeg_in(n_neurons, 0);
+    for (int64_t k = 0; k < m; ++k) {
+        in_ptr[tgt[k] + 1]++;
+        if (pops[pop_of[src[k]]].kind == KIND_INPUT) indeg_in[tgt[k]]++;
+    }
+    for (int64_t i = 0; i < n_neurons; ++i) in_ptr[i + 1] += in_ptr[i];
+    std::vector<int64_t> tord(ord);  // already by spos; stable partition by (target, plastic first)
+    std::stable_sort(tord.begin(), tord.end(), [&](int64_t a, int64_t b) {
+        if (tgt[a] != tgt[b]) return tgt[a] < tgt[b];
+        return (rule[a] >= 0) > (rule[b] >= 0);
+    });
+    tpos_of.assign(m, 0);
+    for (int64_t t = 0; t < m; ++t) tpos_of[tord[t]] = t;
+    for (int64_t i = 0; i < n_neurons; ++i) {
+        int64_t e = in_ptr[i];
+        while (e < in_ptr[i + 1] && rule[tord[e]] >= 0) ++e;
+        plastic_end[i] = e;
+    }
+    // source-major device arrays
+    std::vector<uint32_t> h_out_tgt(m), h_out_tpos(m);
+    std::vector<uint16_t> h_out_units(m);
+    for (int64_t s = 0; s < m; ++s) {
+        int64_t k = ord[s];
+        h_out_tgt[s] = (uint32_t)tgt[k];
+        h_out_tpos[s] = (uint32_t)tpos_of[k];
+        h_out_units[s] = (uint16_t)units[k];
+    }
+    std::vector<int64_t> grp_ptr(n_neurons + 1, 0);
+    std::vector<uint16_t> grp_units;
+    for (int64_t i = 0; i < n_neurons; ++i) {
+        grp_ptr[i] = (int64_t)grp_units.size();
+        for (int64_t s = out_ptr[i]; s < out_ptr[i + 1]; ++s)
+            if (s == out_ptr[i] || h_out_units[s] != h_out_units[s - 1]) grp_units.push_back(h_out_units[s]);
+    }
+    grp_ptr[n_neurons] = (int64_t)grp_units.size();
+    // target-major device arrays
+    std::vector<float> h_w(m), h_maxw(m);
+    std::vector<uint8_t> h_type(m);
+    std::vector<int8_t> h_rule(m);
+    for (int64_t t = 0; t < m; ++t) {
+        int64_t k = tord[t];
+        h_w[t] = weight[k];
+        h_maxw[t] = max_weight[k];
+        h_type[t] = (uint8_t)stype[k];
+        h_rule[t] = (int8_t)rule[k];
+    }
+    // bucket capacities
+    std::vector<uint32_t> h_cap(n_neurons);
+    std::vector<int64_t> h_cap_base(n_neurons);
+    int64_t cap_total = 0;
+    for (int64_t i = 0; i < n_neurons; ++i) {
+        int64_t indeg = in_ptr[i + 1] - in_ptr[i];
+        int64_t c = (indeg - indeg_in[i]) + (int64_t)input_multiplicity * indeg_in[i];
+        c = std::min<int64_t>(c, (int64_t)bucket_limit);
+        h_cap[i] = (uint32_t)c;
+        h_cap_base[i] = cap_total;
+        cap_total += c;
+    }
+    // delay ring: arrival at most ceil(max delay / dt) + 1 steps ahead
+    const double dmax = (double)max_units * 0.0001;
+    R = (int)std::ceil(dmax / dt_s) + 3;
+
+    int rc;
+    cudaStream_t st = stream;
+    NetDev N;
+    memset(&N, 0, sizeof(N));
+    N.n_neurons = n_neurons;
+    N.R = R;
+    if ((rc = dalloc((void **)&d_step, sizeof(int64_t)))) return rc;
+    CK(cudaMemsetAsync(d_step, 0, sizeof(int64_t), st));
+    N.step = d_step;
+    if ((rc = dalloc((void **)&N.cnt, sizeof(uint32_t) * (size_t)R * n_neurons))) return rc;
+    CK(cudaMemsetAsync(N.cnt, 0, sizeof(uint32_t) * (size_t)R * n_neurons, st));
+    if ((rc = dalloc((void **)&N.rec, sizeof(Arrival) * (size_t)R * std::max<int64_t>(cap_total, 1)))) return rc;
+    N.cap_total = cap_total;
+    if ((rc = upload(this, (int64_t **)&N.cap_base, h_cap_base))) return rc;
+    if ((rc = upload(this, (uint32_t **)&N.cap, h_cap))) return rc;
+    if ((rc = upload(this, (int64_t **)&N.out_ptr, out_ptr))) return rc;
+    if ((rc = upload(this, (uint32_t **)&N.out_tgt, h_out_tgt))) return rc;
+    if ((rc = upload(this, (uint32_t **)&N.out_tpos, h_out_tpos))) return rc;
+    if ((rc = upload(this, (uint16_t **)&N.out_units, h_out_units))) return rc;
+    if ((rc = upload(this, (int64_t **)&N.grp_ptr, grp_ptr))) return rc;
+    if ((rc = upload(this, (uint16_t **)&N.grp_units, grp_units))) return rc;
+    if ((rc = upload(this, (int64_t **)&N.in_ptr, in_ptr))) return rc;
+    if ((rc = upload(this, (int64_t **)&N.plastic_end, plastic_end))) return rc;
+    if ((rc = upload(this, &N.w, h_w))) return rc;
+    d_w = N.w;
+    if ((rc = upload(this, (float **)&N.maxw, h_maxw))) return rc;
+    if ((rc = upload(this, (uint8_t **)&N.stype, h_type))) return rc;
+    if ((rc = upload(this, (int8_t **)&N.rule, h_rule))) return rc;
+    std::vector<float> zf(m, 0.0f);
+    std::vector<double> zd(m, 0.0);
+    if ((rc = upload(this, &N.pre, zf))) return rc;
+    if ((rc = upload(this, &N.post, zf))) return rc;
+    if ((rc = upload(this, &N.last, zd))) return rc;
+    std::vector<float> rp;
+    for (auto &r : rules) {
+        rp.push_back(r[0]); rp.push_back(r[1]); rp.push_back(r[2]); rp.push_back(r[3]);
+        rp.push_back(1.0f / r[1]);  // inv_LTPTau = 1.0f/tau (STDPState.cpp:23-26)
+        rp.push_back(1.0f / r[3]);
+    }
+    if (rp.empty()) rp.assign(6, 0.0f);
+    if ((rc = upload(this, (float **)&N.rule_par, rp))) return rc;
+    if ((rc = upload(this, (float **)&N.exp_table, make_exp_table()))) return rc;
+    N.expt_aux = exp_table_aux();
+    if ((rc = dalloc((void **)&N.flags, sizeof(uint32_t)))) return rc;
+    CK(cudaMemsetAsync(N.flags, 0, sizeof(uint32_t), st));
+    if ((rc = dalloc((void **)&N.events, sizeof(unsigned long long)))) return rc;
+    CK(cudaMemsetAsync(N.events, 0, sizeof(unsigned long long), st));
+    if ((rc = dalloc((void **)&N.rec_count, sizeof(unsigned long long)))) return rc;
+    CK(cudaMemsetAsync(N.rec_count, 0, sizeof(unsigned long long), st));
+    N.rec_cap = rec_cap;
+    if (rec_cap > 0 && (rc = dalloc((void **)&N.rec_buf, sizeof(unsigned long long) * (size_t)rec_cap))) return rc;
+    has_inputs = false;
+    for (auto &p : pops)
+        if (p.kind == KIND_INPUT) has_inputs = true;
+    net = N;
+
+    // populations
+    for (auto &p : pops) {
+        if (p.kind == KIND_INPUT) continue;
+        PopDev &D = p.dev;
+        memset(&D, 0, sizeof(D));
+        D.kind = p.kind;
+        D.integ = p.integ;
+        D.bdf_order = p.bdf_order;
+        D.ndiff = model_nd(p.kind);
+        D.nvars = model_nv(p.kind);
+        D.en = p.en;
+        D.first = p.first;
+        D.n = p.n;
+        for (size_t j = 0; j < p.params.size(); ++j) D.p[j] = p.params[j];
+        D.dt_s = p.dt;
+        D.dt_ms = p.dt * 1000.0f;  // IntegrationMethodFast.h:192
+        const float *pr = p.params.data();
+        float tau[3] = {0, 0, 0};
+        float init[kMaxVars] = {0};
+        std::vector<float> nmda;
+        if (p.kind == KIND_LIF) {
+            D.inv_c_m = inv_double(pr[4]);
+            tau[0] = pr[5]; tau[1] = pr[6]; tau[2] = pr[9];
+            init[0] = pr[2];
+            nmda = make_nmda_table(pr[0], pr[1], &D.nmda_aux);
+        } else if (p.kind == KIND_ADEX) {
+            D.inv_c_m = inv_double(pr[10]);
+            D.inv_slope = inv_double(pr[2]);
+            D.inv_tau_w = inv_double(pr[4]);
+            tau[0] = pr[11]; tau[1] = pr[12]; tau[2] = pr[13];
+            init[0] = pr[8];
+            nmda = make_nmda_table(pr[5], pr[6], &D.nmda_aux);
+        } else {
+            D.inv_c_m = inv_double(pr[4]);
+            tau[0] = pr[6]; tau[1] = pr[7]; tau[2] = pr[8];
+            std::vector<float> hh = make_hh_table(pr[5]);
+            D.hh_aux = hh_table_aux();
+            // HHTimeDrivenModel::InitializeStates (HHTimeDrivenModel.cpp:141-166)
+            int pos = (int)((pr[2] - (-90.0f)) * D.hh_aux);
+            if (pos < 0) pos = 0; else if (pos > kHHTable - 1) pos = kHHTable - 1;
+            const float *v = hh.data() + (size_t)pos * 6;
+            init[0] = pr[2];
+            init[1] = v[0] / (v[0] + v[1]);
+            init[2] = v[2] / (v[2] + v[3]);
+            init[3] = v[4] / (v[4] + v[5]);
+            if ((rc = upload(this, (float **)&D.hh_table, hh))) return rc;
+            nmda = make_nmda_table(pr[0], pr[1], &D.nmda_aux);
+        }
+        if ((rc = upload(this, (float **)&D.nmda_table, nmda))) return rc;
+        const float el = (p.integ == INTEG_RK4) ? D.dt_ms * 0.5f : D.dt_ms;  // RK4.h:362
+        for (int c = 0; c < 3; ++c) D.decay[c] = decay_factor(el, tau[c]);
+        bdf_coefficients(D.bdf_coef);
+        memcpy(D.init, init, sizeof(init));
+        D.expt_aux = exp_table_aux();
+        D.exp_table = N.exp_table;
+        const int nd = D.ndiff;
+        for (int v = 0; v < D.nvars; ++v) {
+            bool stored = v < nd || (p.en & (1 << (v - nd)));
+            if (!stored) { D.x[v] = nullptr; continue; }
+            std::vector<float> h(p.n, init[v]);
+            if ((rc = upload(this, &D.x[v], h))) return rc;
+        }
+        if (p.kind == KIND_LIF) {
+            std::vector<int32_t> h(p.n, -1);
+            if ((rc = upload(this, &D.refr, h))) return rc;
+        }
+        if (p.integ == INTEG_BDF) {
+            std::vector<int8_t> hs(p.n, 0);
+            if ((rc = upload(this, &D.bdf_state, hs))) return rc;
+            std::vector<float> hd((size_t)p.bdf_order * nd * p.n, 0.0f);
+            if ((rc = upload(this, &D.bdf_D, hd))) return rc;
+            std::vector<float> hp((size_t)std::max(p.bdf_order - 1, 1) * nd * p.n, 0.0f);
+            if ((rc = upload(this, &D.bdf_P, hp))) return rc;
+        }
+        if ((rc = dalloc((void **)&D.spk, sizeof(uint32_t) * (size_t)p.n))) return rc;
+        if ((rc = dalloc((void **)&D.spk_count, 2 * sizeof(uint32_t)))) return rc;
+        CK(cudaMemsetAsync(D.spk_count, 0, 2 * sizeof(uint32_t), st));
+        uint32_t maxcap = 0;
+        int64_t max_plastic = 0;
+        for (int64_t i = p.first; i < p.first + p.n; ++i) {
+            maxcap = std::max(maxcap, h_cap[i]);
+            max_plastic = std::max(max_plastic, plastic_end[i] - in_ptr[i]);
+        }
+        D.wide = maxcap > 16 ? 1 : 0;
+        p.has_plastic_in = max_plastic > 0;
+        p.post_chunks = (int)((max_plastic + kPostChunk - 1) / kPostChunk);
+        p.has_out = false;
+        for (int64_t i = p.first; i < p.first + p.n; ++i)
+            if (out_ptr[i + 1] > out_ptr[i]) { p.has_out = true; break; }
+    }
+    // dynamic state copied by eb_snapshot / eb_restore
+    dyn.clear();
+    dyn.push_back({d_step, sizeof(int64_t)});
+    dyn.push_back({net.cnt, sizeof(uint32_t) * (size_t)R * n_neurons});
+    dyn.push_back({net.rec, sizeof(Arrival) * (size_t)R * std::max<int64_t>(net.cap_total, 1)});
+    dyn.push_back({net.w, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
+    dyn.push_back({net.pre, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
+    dyn.push_back({net.post, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
+    dyn.push_back({net.last, sizeof(double) * (size_t)std::max<int64_t>(m, 1)});
+    dyn.push_back({net.events, sizeof(unsigned long long)});
+    for (auto &p : pops) {
+        if (p.kind == KIND_INPUT) continue;
+        for (int v = 0; v < p.dev.nvars; ++v)
+            if (p.dev.x[v]) dyn.push_back({p.dev.x[v], sizeof(float) * (size_t)p.n});
+        if (p.dev.refr) dyn.push_back({p.dev.refr, sizeof(int32_t) * (size_t)p.n});
+        if (p.dev.bdf_state) {
+            const int nd = p.dev.ndiff;
+            dyn.push_back({p.dev.bdf_state, sizeof(int8_t) * (size_t)p.n});
+            dyn.push_back({p.dev.bdf_D, sizeof(float) * (size_t)p.bdf_order * nd * p.n});
+            dyn.push_back({p.dev.bdf_P, sizeof(float) * (size_t)std::max(p.bdf_order - 1, 1) * nd * p.n});
+        }
+        dyn.push_back({p.dev.spk_count, 2 * sizeof(uint32_t)});
+    }
+    CK(cudaStreamSynchronize(st));
+    finalized = true;
+    steps_done = 0;
+    // time grid and input bookkeeping
+    t_host.assign(1, 0.0);
+    in_start_host.assign(2, 0);
+    return EB_OK;
+}
+
+// --------------------------------------------------------------- run loop --
+// Grow the device step-time table and input-range table to cover step kmax.
+int eb_ctx::ensure_tables(int64_t kmax) {
+    while ((int64_t)t_host.size() <= kmax) {
+        double t = t_host.back() + (double)dt_f;  // TimeEventUpdateNeurons.cpp:115
+        t_host.push_back(t);
+    }
+    int64_t need = kmax + 1;
+    if (need > tcap) {
+        int64_t ncap = std::max<int64_t>(need * 2, 4096);
+        double *nt = nullptr;
+        int64_t *ni = nullptr;
+        int rc;
+        if ((rc = dalloc((void **)&nt, sizeof(double) * (size_t)ncap))) return rc;
+        if ((rc = dalloc((void **)&ni, sizeof(int64_t) * (size_t)(ncap + 1)))) return rc;
+        CK(cudaMemsetAsync(ni, 0, sizeof(int64_t) * (size_t)(ncap + 1), stream));
+        if (d_instart && tcap > 0)
+            CK(cudaMemcpyAsync(ni, d_instart, sizeof(int64_t) * (size_t)(tcap + 1), cudaMemcpyDeviceToDevice, stream));
+        d_tstep = nt;
+        d_instart = ni;
+        tcap = ncap;
+        tstep_uploaded = 0;
+        graphs_valid = false;
+    }
+    if (tstep_uploaded < need) {
+        CK(cudaMemcpyAsync(d_tstep + tstep_uploaded, t_host.data() + tstep_uploaded,
+                           sizeof(double) * (size_t)(need - tstep_uploaded), cudaMemcpyHostToDevice, stream));
+        tstep_uploaded = need;
+    }
+    net.tstep = d_tstep;
+    net.in_start = d_instart;
+    return EB_OK;
+}
+
+// Move pending input spikes with time < t_{k_end} to the device and fill the
+// input ranges of steps k0+1 .. k_end+1.
+int eb_ctx::stage_inputs(int64_t k0, int64_t k_end) {
+    const double tend = t_host[k_end];
+    std::vector<double> nt;
+    std::vector<uint32_t> nc;
+    std::vector<PendingIn> rest;
+    for (auto &p : pending) {
+        if ((double)p.t < tend) { nt.push_back((double)p.t); nc.push_back((uint32_t)p.cell); }
+        else rest.push_back(p);
+    }
+    pending.swap(rest);
+    if (!nt.empty()) {
+        int64_t need = in_total + (int64_t)nt.size();
+        if (need > in_cap) {
+            int64_t ncap = std::max<int64_t>(need * 2, 1 << 16);
+            double *dt = nullptr;
+            uint32_t *dc = nullptr;
+            int rc;
+            if ((rc = dalloc((void **)&dt, sizeof(double) * (size_t)ncap))) return rc;
+            if ((rc = dalloc((void **)&dc, sizeof(uint32_t) * (size_t)ncap))) return rc;
+            if (in_total) {
+                CK(cudaMemcpyAsync(dt, d_in_time, sizeof(double) * (size_t)in_total, cudaMemcpyDeviceToDevice, stream));
+                CK(cudaMemcpyAsync(dc, d_in_cell, sizeof(uint32_t) * (size_t)in_total, cudaMemcpyDeviceToDevice, stream));
+            }
+            d_in_time = dt;
+            d_in_cell = dc;
+            in_cap = ncap;
+            graphs_valid = false;
+        }
+        CK(cudaMemcpyAsync(d_in_time + in_total, nt.data(), sizeof(double) * nt.size(), cudaMemcpyHostToDevice, stream));
+        CK(cudaMemcpyAsync(d_in_cell + in_total, nc.data(), sizeof(uint32_t) * nc.size(), cudaMemcpyHostToDevice, stream));
+        in_times_host.insert(in_times_host.end(), nt.begin(), nt.end());
+        in_total += (int64_t)nt.size();
+    }
+    // in_start[k] = first staged input with time >= t_{k-1}
+    std::vector<int64_t> h(k_end - k0 + 1);
+    for (int64_t k = k0 + 1; k <= k_end + 1; ++k) {
+        double lo = t_host[k - 1];
+        h[k - k0 - 1] = std::lower_bound(in_times_host.begin(), in_times_host.end(), lo) - in_times_host.begin();
+    }
+    CK(cudaMemcpyAsync(d_instart + k0 + 1, h.data(), sizeof(int64_t) * h.size(), cudaMemcpyHostToDevice, stream));
+    net.in_time = d_in_time;
+    net.in_cell = d_in_cell;
+    return EB_OK;
+}
+
+void eb_ctx::enqueue_step(int rel) {
+    const int fan_blocks = 148 * 2;
+    if (has_inputs) launch_input_push(net, rel, dt_s, fan_blocks, stream);
+    for (auto &p : pops)
+        if (p.kind != KIND_INPUT) launch_update(p.dev, net, rel, stream);
+    for (auto &p : pops) {
+        if (p.kind == KIND_INPUT) continue;
+        if (p.has_plastic_in)
+            launch_post_stdp(p.dev, net, rel, kPostChunk, p.post_chunks, fan_blocks, stream);
+        if (p.has_out) launch_push(p.dev, net, rel, dt_s, fan_blocks, stream);
+    }
+}
+
+int eb_ctx::build_graph(int K) {
+    if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int r = 0; r < K; ++r) enqueue_step(r);
+    launch_advance(d_step, K, stream);
+    CK(cudaStreamEndCapture(stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e)); return EB_ERR_CUDA; }
+    graph_K = K;
+    graphs_valid = true;
+    return EB_OK;
+}
+
+int eb_ctx::run_async(int64_t n) {
+    if (!finalized) { set_error("eb_run before eb_finalize"); return EB_ERR_STATE; }
+    if (n <= 0) return EB_OK;
+    const int64_t k0 = steps_done, k_end = k0 + n;
+    int rc;
+    if ((rc = ensure_tables(k_end + R + 8))) return rc;
+    if ((rc = stage_inputs(k0, k_end))) return rc;
+    if (trace_pending) {
+        net.trace_k0 = k0 + 1;
+        trace_pending = false;
+        graphs_valid = false;
+    }
+    int K = graph_steps > 0 ? graph_steps : 64;
+    int64_t done = 0;
+    if (K > 1 && n >= K) {
+        if (!graphs_valid || graph_K != K)
+            if ((rc = build_graph(K))) return rc;
+        while (n - done >= K) {
+            CK(cudaGraphLaunch(graph_exec, stream));
+            done += K;
+        }
+    }
+    while (done < n) {
+        enqueue_step(0);
+        launch_advance(d_step, 1, stream);
+        done++;
+    }
+    CK(cudaGetLastError());
+    steps_done = k_end;
+    return EB_OK;
+}
+
+int eb_ctx::sync() {
+    CK(cudaStreamSynchronize(stream));
+    uint32_t f = 0;
+    CK(cudaMemcpy(&f, net.flags, sizeof(f), cudaMemcpyDeviceToHost));
+    if (f) {
+        CK(cudaMemset(net.flags, 0, sizeof(uint32_t)));
+        if (f & FLAG_BDF_SINGULAR) { set_error("BDF Newton matrix not invertible"); return EB_ERR_NUMERIC; }
+        if (f & FLAG_BUCKET_OVERFLOW) {
+            set_error("arrival bucket overflow: a neuron received more spikes in one step than its bucket holds "
+                      "(raise eb_set_bucket_limit)");
+            return EB_ERR_OVERFLOW;
+        }
+        if (f & FLAG_RECORD_OVERFLOW) { set_error("spike recording buffer full (drain with eb_get_spikes or raise eb_set_record_capacity)"); return EB_ERR_OVERFLOW; }
+        if (f & FLAG_SPIKELIST_OVERFLOW) { set_error("internal spike list overflow"); return EB_ERR_OVERFLOW; }
+    }
+    return EB_OK;
+}
+
+int eb_ctx::snapshot(int slot) {
+    if (!finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    std::vector<void *> *bufs = nullptr;
+    for (auto &s : snapshots)
+        if (s.first == slot) bufs = &s.second;
+    if (!bufs) {
+        snapshots.push_back({slot, {}});
+        bufs = &snapshots.back().second;
+        for (auto &d : dyn) {
+            void *p = nullptr;
+            int rc = dalloc(&p, d.second);
+            if (rc) return rc;
+            bufs->push_back(p);
+        }
+    }
+    for (size_t i = 0; i < dyn.size(); ++i)
+        CK(cudaMemcpyAsync((*bufs)[i], dyn[i].first, dyn[i].second, cudaMemcpyDeviceToDevice, stream));
+    bool found = false;
+    for (auto &h : snap_host)
+        if (h.slot == slot) { h.steps_done = steps_done; h.spikes_drained = spikes_drained; found = true; }
+    if (!found) snap_host.push_back({slot, steps_done, spikes_drained});
+    CK(cudaStreamSynchronize(stream));
+    return EB_OK;
+}
+
+int eb_ctx::restore(int slot) {
+    std::vector<void *> *bufs = nullptr;
+    for (auto &s : snapshots)
+        if (s.first == slot) bufs = &s.second;
+    if (!bufs) { set_error("no snapshot in slot %d", slot); return EB_ERR_STATE; }
+    for (size_t i = 0; i < dyn.size(); ++i)
+        CK(cudaMemcpyAsync(dyn[i].first, (*bufs)[i], dyn[i].second, cudaMemcpyDeviceToDevice, stream));
+    for (auto &h : snap_host)
+        if (h.slot == slot) { steps_done = h.steps_done; }
+    CK(cudaMemsetAsync(net.rec_count, 0, sizeof(unsigned long long), stream));
+    CK(cudaStreamSynchronize(stream));
+    return EB_OK;
+}
+
+eb_ctx::~eb_ctx() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    dfree_all();
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+// ================================================================== C ABI ==
+extern "C" {
+
+const char *eb_last_error(void) { return g_err.c_str(); }
+const char *eb_version(void) { return "edlut_b200 0.1 (sm_100a)"; }
+
+int eb_ctx_create(int device, void *stream, eb_ctx **out) {
+    if (!out) { set_error("null out"); return EB_ERR_ARG; }
+    *out = nullptr;
+    CK(cudaSetDevice(device));
+    eb_ctx *c = new eb_ctx();
+    c->device = device;
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+        c->own_stream = false;
+    } else {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) { delete c; set_error("cudaStreamCreate: %s", cudaGetErrorString(e)); return EB_ERR_CUDA; }
+        c->own_stream = true;
+    }
+    *out = c;
+    return EB_OK;
+}
+
+int eb_ctx_destroy(eb_ctx *ctx) {
+    if (!ctx) return EB_OK;
+    cudaSetDevice(ctx->device);
+    delete ctx;
+    return EB_OK;
+}
+
+int eb_add_population(eb_ctx *ctx, int kind, int64_t n, int integrator, int bdf_order, float dt_s,
+                      const float *params, int n_params, int64_t *out_first) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    return ctx->add_population(kind, n, integrator, bdf_order, dt_s, params, n_params, out_first);
+}
+
+int eb_add_stdp_rule(eb_ctx *ctx, float max_ltp, float tau_ltp, float max_ltd, float tau_ltd, int *out_rule) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (ctx->finalized) { set_error("eb_add_stdp_rule after eb_finalize"); return EB_ERR_STATE; }
+    if (!(tau_ltp > 0) || !(tau_ltd > 0)) { set_error("STDP time constants must be > 0"); return EB_ERR_ARG; }
+    ctx->rules.push_back({max_ltp, tau_ltp, max_ltd, tau_ltd});
+    if (out_rule) *out_rule = (int)ctx->rules.size() - 1;
+    return EB_OK;
+}
+
+int eb_set_connectivity(eb_ctx *ctx, int64_t m, const int64_t *src, const int64_t *tgt, const float *delay_s,
+                        const int32_t *type, const float *weight, const float *max_weight, const int32_t *rule) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (ctx->finalized) { set_error("eb_set_connectivity after eb_finalize"); return EB_ERR_STATE; }
+    if (m < 0 || (m > 0 && (!src || !tgt || !delay_s || !type || !weight || !max_weight))) {
+        set_error("bad connectivity arrays");
+        return EB_ERR_ARG;
+    }
+    if (m >= (int64_t)UINT32_MAX) { set_error("more than 2^32-1 synapses"); return EB_ERR_UNSUPPORTED; }
+    ctx->src.assign(src, src + m);
+    ctx->tgt.assign(tgt, tgt + m);
+    ctx->delay.assign(delay_s, delay_s + m);
+    ctx->stype.assign(type, type + m);
+    ctx->weight.assign(weight, weight + m);
+    ctx->max_weight.assign(max_weight, max_weight + m);
+    if (rule) ctx->rule.assign(rule, rule + m);
+    else ctx->rule.assign(m, -1);
+    return EB_OK;
+}
+
+int eb_set_bucket_limit(eb_ctx *ctx, uint32_t max_per_target, uint32_t input_multiplicity) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (ctx->finalized) { set_error("eb_set_bucket_limit after eb_finalize"); return EB_ERR_STATE; }
+    if (max_per_target) ctx->bucket_limit = max_per_target;
+    if (input_multiplicity) ctx->input_multiplicity = input_multiplicity;
+    return EB_OK;
+}
+
+int eb_finalize(eb_ctx *ctx, int64_t *out_sorted_perm) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    CK(cudaSetDevice(ctx->device));
+    return ctx->finalize(out_sorted_perm);
+}
+
+int eb_inject_spikes(eb_ctx *ctx, int64_t n, const float *time_s, const int64_t *cell) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (n < 0 || (n > 0 && (!time_s || !cell))) { set_error("bad input arrays"); return EB_ERR_ARG; }
+    double now = ctx->finalized && !ctx->t_host.empty() ? ctx->t_host[std::min<int64_t>(ctx->steps_done, (int64_t)ctx->t_host.size() - 1)] : 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (cell[i] < 0 || cell[i] >= ctx->n_neurons) { set_error("input spike %lld: neuron out of range", (long long)i); return EB_ERR_ARG; }
+        if ((double)time_s[i] < now || !(time_s[i] >= 0.0f)) {
+            set_error("input spike %lld at %g s precedes the simulation time %g s", (long long)i, (double)time_s[i], now);
+            return EB_ERR_ARG;
+        }
+    }
+    for (int64_t i = 0; i < n; ++i) ctx->pending.push_back({time_s[i], cell[i], ctx->pending_seq++});
+    std::stable_sort(ctx->pending.begin(), ctx->pending.end(), [](const PendingIn &a, const PendingIn &b) {
+        if (a.t != b.t) return a.t < b.t;
+        return a.seq < b.seq;
+    });
+    return EB_OK;
+}
+
+int eb_set_graph_steps(eb_ctx *ctx, int graph_steps) {
+    if (!ctx || graph_steps < 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    ctx->graph_steps = graph_steps;
+    return EB_OK;
+}
+
+int eb_run_async(eb_ctx *ctx, int64_t n_steps) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    CK(cudaSetDevice(ctx->device));
+    return ctx->run_async(n_steps);
+}
+
+int eb_sync(eb_ctx *ctx) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    return ctx->sync();
+}
+
+int eb_run(eb_ctx *ctx, int64_t n_steps) {
+    int rc = eb_run_async(ctx, n_steps);
+    if (rc) return rc;
+    return ctx->sync();
+}
+
+int eb_set_record_capacity(eb_ctx *ctx, int64_t cap) {
+    if (!ctx || cap < 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (ctx->finalized) { set_error("eb_set_record_capacity after eb_finalize"); return EB_ERR_STATE; }
+    ctx->rec_cap = cap;
+    return EB_OK;
+}
+
+int eb_get_spikes(eb_ctx *ctx, int64_t cap, int64_t *n, int64_t *step, int64_t *cell) {
+    if (!ctx || !n) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long cnt = 0;
+    CK(cudaMemcpy(&cnt, ctx->net.rec_count, sizeof(cnt), cudaMemcpyDeviceToHost));
+    int64_t have = (int64_t)std::min<unsigned long long>(cnt, (unsigned long long)ctx->rec_cap);
+    *n = have;
+    if (have > cap) { set_error("eb_get_spikes: %lld spikes, buffer holds %lld", (long long)have, (long long)cap); return EB_ERR_OVERFLOW; }
+    std::vector<unsigned long long> h(have);
+    if (have) CK(cudaMemcpy(h.data(), ctx->net.rec_buf, sizeof(unsigned long long) * (size_t)have, cudaMemcpyDeviceToHost));
+    std::sort(h.begin(), h.end());
+    for (int64_t i = 0; i < have; ++i) {
+        if (step) step[i] = (int64_t)(h[i] >> 32);
+        if (cell) cell[i] = (int64_t)(h[i] & 0xffffffffull);
+    }
+    ctx->spikes_drained += have;
+    CK(cudaMemset(ctx->net.rec_count, 0, sizeof(unsigned long long)));
+    return EB_OK;
+}
+
+int eb_step_time(eb_ctx *ctx, int64_t k, double *t) {
+    if (!ctx || !t || k < 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    while ((int64_t)ctx->t_host.size() <= k) ctx->t_host.push_back(ctx->t_host.back() + (double)ctx->dt_f);
+    *t = ctx->t_host[k];
+    return EB_OK;
+}
+
+static int state_io(eb_ctx *ctx, int64_t first, int64_t n, int var, float *buf, bool get) {
+    if (!ctx || n < 0 || first < 0 || first + n > ctx->n_neurons || var < 0 || var >= kMaxVars) {
+        set_error("bad state range");
+        return EB_ERR_ARG;
+    }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    int64_t i = first, end = first + n;
+    while (i < end) {
+        const HostPop &p = ctx->pops[ctx->pop_of[i]];
+        int64_t e = std::min(end, p.first + p.n);
+        int64_t off = i - p.first, cnt = e - i;
+        float *dst = buf + (i - first);
+        if (p.kind == KIND_INPUT || var >= p.dev.nvars || !p.dev.x[var]) {
+            if (get) std::fill(dst, dst + cnt, 0.0f);
+            else if (p.kind != KIND_INPUT && var < p.dev.nvars) { set_error("state variable %d is not stored", var); return EB_ERR_ARG; }
+        } else if (get) {
+            CK(cudaMemcpy(dst, p.dev.x[var] + off, sizeof(float) * (size_t)cnt, cudaMemcpyDeviceToHost));
+        } else {
+            CK(cudaMemcpy(p.dev.x[var] + off, dst, sizeof(float) * (size_t)cnt, cudaMemcpyHostToDevice));
+        }
+        i = e;
+    }
+    return EB_OK;
+}
+
+int eb_get_state(eb_ctx *ctx, int64_t first, int64_t n, int var, float *out) {
+    return state_io(ctx, first, n, var, out, true);
+}
+int eb_set_state(eb_ctx *ctx, int64_t first, int64_t n, int var, const float *in) {
+    return state_io(ctx, first, n, var, const_cast<float *>(in), false);
+}
+
+int eb_set_trace(eb_ctx *ctx, int64_t first, int64_t n, int64_t steps) {
+    if (!ctx || first < 0 || n < 0 || steps < 0 || first + n > ctx->n_neurons) { set_error("bad trace range"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    size_t bytes = sizeof(float) * (size_t)n * (size_t)steps * kMaxVars;
+    if (bytes > ctx->trace_bytes) {
+        int rc = ctx->dalloc((void **)&ctx->net.trace, bytes);
+        if (rc) return rc;
+        ctx->trace_bytes = bytes;
+    }
+    if (bytes) CK(cudaMemsetAsync(ctx->net.trace, 0, bytes, ctx->stream));
+    ctx->net.trace_first = first;
+    ctx->net.trace_n = n;
+    ctx->net.trace_steps = steps;
+    ctx->trace_pending = true;
+    ctx->graphs_valid = false;
+    return EB_OK;
+}
+
+int eb_get_trace(eb_ctx *ctx, float *out) {
+    if (!ctx || !out) { set_error("bad argument"); return EB_ERR_ARG; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    size_t bytes = sizeof(float) * (size_t)ctx->net.trace_n * (size_t)ctx->net.trace_steps * kMaxVars;
+    if (bytes) CK(cudaMemcpy(out, ctx->net.trace, bytes, cudaMemcpyDeviceToHost));
+    return EB_OK;
+}
+
+int eb_get_weights(eb_ctx *ctx, float *w) {
+    if (!ctx || !w) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int64_t m = (int64_t)ctx->src.size();
+    std::vector<float> h(m);
+    if (m) CK(cudaMemcpy(h.data(), ctx->d_w, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < m; ++k) w[k] = h[ctx->tpos_of[k]];
+    return EB_OK;
+}
+
+int eb_set_weights(eb_ctx *ctx, const float *w) {
+    if (!ctx || !w) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    const int64_t m = (int64_t)ctx->src.size();
+    std::vector<float> h(m);
+    for (int64_t k = 0; k < m; ++k) h[ctx->tpos_of[k]] = w[k];
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (m) CK(cudaMemcpy(ctx->d_w, h.data(), sizeof(float) * (size_t)m, cudaMemcpyHostToDevice));
+    return EB_OK;
+}
+
+int eb_get_counters(eb_ctx *ctx, int64_t *steps, int64_t *spikes, int64_t *events) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long ev = 0, rc = 0;
+    CK(cudaMemcpy(&ev, ctx->net.events, sizeof(ev), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&rc, ctx->net.rec_count, sizeof(rc), cudaMemcpyDeviceToHost));
+    if (steps) *steps = ctx->steps_done;
+    if (spikes) *spikes = ctx->spikes_drained + (int64_t)rc;
+    if (events) *events = (int64_t)ev;
+    return EB_OK;
+}
+
+int eb_snapshot(eb_ctx *ctx, int slot) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    return ctx->snapshot(slot);
+}
+
+int eb_restore(eb_ctx *ctx, int slot) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    return ctx->restore(slot);
+}
+
+int eb_device_bytes(eb_ctx *ctx, int64_t *bytes) {
+    if (!ctx || !bytes) { set_error("bad argument"); return EB_ERR_ARG; }
+    *bytes = ctx->dev_bytes;
+    return EB_OK;
+}
+
+}  // extern "C"

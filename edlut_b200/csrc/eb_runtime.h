@@ -1,0 +1,106 @@
+// Host-side context of the device-resident network (eb_runtime.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "eb_types.h"
+
+namespace eb {
+
+void set_error(const char *fmt, ...);
+
+constexpr int kPostChunk = 2048;  // plastic synapses per post-STDP work item
+
+struct HostPop {
+    int kind = KIND_INPUT, integ = 0, bdf_order = 0;
+    int64_t n = 0, first = 0;
+    float dt = 0.0f;
+    std::vector<float> params;
+    int en = 0;                 // enabled conductance types (from the synapse types targeting it)
+    bool has_out = false, has_plastic_in = false;
+    int post_chunks = 1;
+    PopDev dev{};
+};
+
+struct PendingIn {
+    float t;
+    int64_t cell;
+    int64_t seq;
+};
+
+}  // namespace eb
+
+struct eb_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // description
+    std::vector<eb::HostPop> pops;
+    int64_t n_neurons = 0;
+    std::vector<std::array<float, 4>> rules;
+    std::vector<int64_t> src, tgt;
+    std::vector<float> delay, weight, max_weight;
+    std::vector<int32_t> stype, rule;
+    uint32_t bucket_limit = 8192, input_multiplicity = 2;
+    int64_t rec_cap = 16 << 20;
+    // derived
+    bool finalized = false;
+    float dt_f = 0.0f;
+    double dt_s = 0.0;
+    int R = 0;
+    std::vector<int> pop_of;
+    std::vector<int64_t> spos_of, tpos_of;
+    eb::NetDev net{};
+    int64_t *d_step = nullptr;
+    float *d_w = nullptr;
+    bool has_inputs = false;
+    // time grid and inputs
+    std::vector<double> t_host;
+    double *d_tstep = nullptr;
+    int64_t *d_instart = nullptr;
+    int64_t tcap = 0, tstep_uploaded = 0;
+    std::vector<int64_t> in_start_host;
+    std::vector<eb::PendingIn> pending;
+    int64_t pending_seq = 0;
+    std::vector<double> in_times_host;
+    double *d_in_time = nullptr;
+    uint32_t *d_in_cell = nullptr;
+    int64_t in_total = 0, in_cap = 0;
+    // run state
+    int64_t steps_done = 0;
+    int64_t spikes_drained = 0;
+    int graph_steps = 0;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_K = 0;
+    bool graph_inputs = false;
+    bool graphs_valid = false;
+    bool trace_pending = false;
+    size_t trace_bytes = 0;
+    // allocations
+    std::vector<void *> allocs;
+    int64_t dev_bytes = 0;
+    // dynamic device state (what a snapshot copies): (pointer, bytes)
+    std::vector<std::pair<void *, size_t>> dyn;
+    std::vector<std::pair<int, std::vector<void *>>> snapshots;
+    struct HostSnap { int slot; int64_t steps_done, spikes_drained; };
+    std::vector<HostSnap> snap_host;
+
+    int dalloc(void **p, size_t bytes);
+    void dfree_all();
+    int add_population(int kind, int64_t n, int integ, int bdf_order, float dt, const float *params, int n_params,
+                       int64_t *out_first);
+    int finalize(int64_t *out_sorted_perm);
+    int ensure_tables(int64_t kmax);
+    int stage_inputs(int64_t k0, int64_t k_end);
+    void enqueue_step(int rel);
+    int build_graph(int K);
+    int run_async(int64_t n);
+    int sync();
+    int snapshot(int slot);
+    int restore(int slot);
+    ~eb_ctx();
+};

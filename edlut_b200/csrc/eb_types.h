@@ -1,0 +1,104 @@
+// Shared host/device types of the edlut_b200 runtime.
+#pragma once
+#include <cstdint>
+
+namespace eb {
+
+enum Kind : int { KIND_INPUT = 0, KIND_LIF = 1, KIND_ADEX = 2, KIND_HH = 3 };
+enum Integ : int { INTEG_EULER = 0, INTEG_RK2 = 1, INTEG_RK4 = 2, INTEG_BDF = 3 };
+
+constexpr int kMaxVars = 8;
+constexpr int kNmdaTable = 256;
+constexpr int kExptTable = 1024 * 16;
+constexpr int kHHTable = 1024 * 256;
+
+// Device error flags (ORed into NetDev::flags).
+constexpr uint32_t FLAG_BUCKET_OVERFLOW = 1u;
+constexpr uint32_t FLAG_BDF_SINGULAR = 2u;
+constexpr uint32_t FLAG_RECORD_OVERFLOW = 4u;
+constexpr uint32_t FLAG_SPIKELIST_OVERFLOW = 8u;
+
+// One delivery waiting in a target's bucket: the arrival time (double seconds,
+// as the reference computes it) and the synapse, both in source-major order
+// (spos, the reference's sorted synapse order, breaks ties) and in the
+// target-major layout (tpos, where weight and plasticity state live).
+struct alignas(16) Arrival {
+    double a;
+    uint32_t spos;
+    uint32_t tpos;
+};
+
+// Per-population parameters, passed by value to the kernels.
+struct PopDev {
+    int kind, integ, bdf_order, ndiff, nvars;
+    int en;          // bit0 EXC, bit1 INH, bit2 NMDA conductances enabled
+    int64_t first;   // first global neuron index
+    int64_t n;       // neurons in the population
+    float p[16];     // model parameters in .cfg order
+    float dt_s, dt_ms;
+    float inv_c_m, inv_slope, inv_tau_w;
+    float decay[3];  // conductance decay factor per step (RK4: per half step)
+    float bdf_coef[7][7];
+    float init[kMaxVars];
+    float expt_aux, hh_aux, nmda_aux;
+    const float *exp_table;
+    const float *hh_table;
+    const float *nmda_table;
+    // state (SoA); x[v] == nullptr for variables that are not stored
+    float *x[kMaxVars];
+    int32_t *refr;       // LIF: updates since last spike (-1 never)
+    int8_t *bdf_state;
+    float *bdf_D, *bdf_P;
+    // spike list (local indices) with a double-buffered count
+    uint32_t *spk;
+    uint32_t *spk_count;  // [2]
+    // in-synapse ranges (target-major) for neurons of this population
+    int wide;            // 1: warp-per-neuron update (large in-degree)
+};
+
+// Network-wide device pointers, passed by value to the kernels.
+struct NetDev {
+    int64_t n_neurons;
+    int R;                       // delay-ring slots
+    const int64_t *step;         // current step counter (steps completed)
+    const double *tstep;         // update times t_k, k = 0..
+    // arrival buckets
+    uint32_t *cnt;               // [R][n_neurons]
+    Arrival *rec;                // [R][cap_total]
+    const int64_t *cap_base;     // [n_neurons] offset of each target's bucket
+    const uint32_t *cap;         // [n_neurons]
+    int64_t cap_total;
+    // source-major synapses (reference order)
+    const int64_t *out_ptr;      // [n_neurons+1]
+    const uint32_t *out_tgt;
+    const uint32_t *out_tpos;
+    const uint16_t *out_units;   // delay in units of 0.1 ms
+    const int64_t *grp_ptr;      // per-source distinct-delay groups [n_neurons+1]
+    const uint16_t *grp_units;
+    // target-major synapses
+    const int64_t *in_ptr;       // [n_neurons+1]
+    const int64_t *plastic_end;  // [n_neurons] end of the plastic prefix of each target's range
+    float *w;
+    const float *maxw;
+    const uint8_t *stype;
+    const int8_t *rule;
+    float *pre, *post;
+    double *last;
+    const float *rule_par;       // [n_rules][6]: max_LTP, tau_LTP, max_LTD, tau_LTD, inv_LTP, inv_LTD
+    const float *exp_table;
+    float expt_aux;
+    // input spikes
+    const double *in_time;
+    const uint32_t *in_cell;
+    const int64_t *in_start;     // [step] first input with time >= t_{step-1}
+    // recording
+    unsigned long long *rec_buf; // (step << 32) | neuron
+    unsigned long long *rec_count;
+    int64_t rec_cap;
+    float *trace;                // [steps][n][kMaxVars]
+    int64_t trace_first, trace_n, trace_k0, trace_steps;
+    unsigned long long *events;  // delivered synaptic events
+    uint32_t *flags;
+};
+
+}  // namespace eb

@@ -1,0 +1,161 @@
+/*
+ * edlut_b200 -- C ABI of the B200 time-driven simulation path.
+ *
+ * Plain C types only (no CUDA or torch types): a host program, a C++ neuron-model
+ * plugin, ctypes or any other FFI binds these symbols from libedlut_b200.so.
+ * All functions return EB_OK (0) or a negative EB_ERR_* code; eb_last_error()
+ * returns a message for the calling thread's last failure.  No C++ exception
+ * crosses this boundary and no function calls exit().
+ *
+ * References are paths in the EDLUT reference tree, relative to its Kernel/
+ * directory.
+ *
+ * Two levels:
+ *  1. Network level (device-resident network): populations, synapses, STDP rules,
+ *     input spikes and K-step runs all on the GPU.  Replaces the per-step host work
+ *     of the reference engine for time-driven networks: TimeEventUpdateNeurons
+ *     (src/simulation/TimeEventUpdateNeurons.cpp:82-116), TimeDrivenInternalSpike
+ *     (src/spike/TimeDrivenInternalSpike.cpp:182-253), PropagatedSpikeGroup delivery
+ *     (src/spike/PropagatedSpikeGroup.cpp:112-149) and the STDP hooks
+ *     (src/learning_rules/STDPWeightChange.cpp:43-76).
+ *  2. Model level (eb_model_*): one time-driven neuron population stepped by a host
+ *     engine, the drop-in for TimeDrivenNeuronModel_GPU_C_INTERFACE
+ *     (include/neuron_model/TimeDrivenNeuronModel_GPU_C_INTERFACE.cuh:64-423).
+ */
+#ifndef EDLUT_B200_H
+#define EDLUT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EB_OK 0
+#define EB_ERR_ARG (-1)        /* bad argument */
+#define EB_ERR_CUDA (-2)       /* CUDA runtime failure */
+#define EB_ERR_STATE (-3)      /* call made in the wrong phase (e.g. run before finalize) */
+#define EB_ERR_OVERFLOW (-4)   /* an arrival bucket, spike list or recording buffer overflowed */
+#define EB_ERR_PARSE (-5)      /* .cfg / network / weights / input file error */
+#define EB_ERR_UNSUPPORTED (-6)/* model, integrator or synapse type outside this path */
+#define EB_ERR_NOMEM (-7)      /* device allocation failed */
+#define EB_ERR_NUMERIC (-8)    /* BDF Newton matrix singular (the reference exits the process) */
+
+/* Neuron model kinds: the reference names LIFTimeDrivenModel[_GPU],
+ * AdExTimeDrivenModel[_GPU], HHTimeDrivenModel[_GPU] and InputSpikeNeuronModel
+ * (src/neuron_model/NeuronModelFactory.cu:85-91,221-257). */
+#define EB_INPUT 0
+#define EB_LIF 1
+#define EB_ADEX 2
+#define EB_HH 3
+/* Integration methods "Euler", "RK2", "RK4", "BDF"
+ * (src/integration_method/IntegrationMethodFactory_GPU_C_INTERFACE.cu:54-97). */
+#define EB_EULER 0
+#define EB_RK2 1
+#define EB_RK4 2
+#define EB_BDF 3
+
+typedef struct eb_ctx eb_ctx;
+
+/* Last error message of the calling thread ("" if none). */
+const char *eb_last_error(void);
+/* Library version string. */
+const char *eb_version(void);
+
+/* ----------------------------------------------------------- lifecycle --- */
+/* Create a context on CUDA device `device`.  `stream` is a cudaStream_t passed as a
+ * pointer (NULL: the library creates its own).  Replaces the per-queue
+ * cudaSetDevice + InitializeStatesGPU set-up, src/neuron_model/LIFTimeDrivenModel_GPU_C_INTERFACE.cu:139-194. */
+int eb_ctx_create(int device, void *stream, eb_ctx **out);
+int eb_ctx_destroy(eb_ctx *ctx);
+
+/* ------------------------------------------------------------- network --- */
+/* Append a population (one layer line of the network file, Network::ParseNet,
+ * src/spike/Network.cpp:448-484).  params: the model's .cfg values in file order
+ * (e.g. LIF: e_exc e_inh e_leak v_thr c_m tau_exc tau_inh tau_ref g_leak tau_nmda,
+ * LIFTimeDrivenModel::ParseNeuronModel); dt_s the integration step in seconds as
+ * parsed (float).  Input populations (EB_INPUT) take no params.  *out_first gets
+ * the population's first global neuron index. */
+int eb_add_population(eb_ctx *ctx, int kind, int64_t n, int integrator, int bdf_order,
+                      float dt_s, const float *params, int n_params, int64_t *out_first);
+/* Additive STDP rule "STDP" with its .cfg values max_LTP tau_LTP max_LTD tau_LTD
+ * (taus in seconds), STDPWeightChange::ParseLearningRule,
+ * src/learning_rules/STDPWeightChange.cpp:78-99.  *out_rule gets its index. */
+int eb_add_stdp_rule(eb_ctx *ctx, float max_ltp, float tau_ltp, float max_ltd, float tau_ltd,
+                     int *out_rule);
+/* Synapses in network-file order (Network::CreateConnections,
+ * src/spike/Network.cpp:790-1014): source, target, delay (s, float as parsed; rounded
+ * like RoundPropagationDelay, :1311-1317), type (0 AMPA, 1 GABA, 2 NMDA), weight,
+ * max weight, learning rule (-1: none).  May be called once. */
+int eb_set_connectivity(eb_ctx *ctx, int64_t m, const int64_t *src, const int64_t *tgt,
+                        const float *delay_s, const int32_t *type, const float *weight,
+                        const float *max_weight, const int32_t *rule);
+/* Per-target bucket capacity limit (arrivals one neuron can take in one step);
+ * default min(in-degree x multiplicity, 8192). */
+int eb_set_bucket_limit(eb_ctx *ctx, uint32_t max_per_target, uint32_t input_multiplicity);
+/* Build the device network: sort synapses (qsort_inters order,
+ * src/spike/Network.cpp:45-68), build source-major and target-major tables, allocate
+ * state, buckets and tables.  *out_sorted_perm (m entries, optional) receives the
+ * reference's synapse order as original indices. */
+int eb_finalize(eb_ctx *ctx, int64_t *out_sorted_perm);
+/* Load a reference network file + weights file (Network::ParseNet,
+ * src/spike/Network.cpp:422-704); equivalent to the calls above.  Model .cfg paths
+ * are resolved like the reference (relative to the current directory, ".cfg" added). */
+int eb_load_network_files(eb_ctx *ctx, const char *network_file, const char *weights_file);
+
+/* --------------------------------------------------------------- inputs --- */
+/* Spikes of input neurons (InputSpikeNeuronModel), times in seconds as float like
+ * FileInputSpikeDriver (src/communication/FileInputSpikeDriver.cpp:45-78) or the
+ * ArrayInputSpikeDriver.  Times must not precede the current simulation time. */
+int eb_inject_spikes(eb_ctx *ctx, int64_t n, const float *time_s, const int64_t *cell);
+/* Load an input-spike file in the reference format. */
+int eb_load_input_file(eb_ctx *ctx, const char *input_file);
+
+/* ----------------------------------------------------------------- run --- */
+/* Advance n_steps integration steps (each: deliveries, neuron updates, spikes, STDP),
+ * replaying captured CUDA graphs of `graph_steps` steps (0: default 64; 1: plain
+ * launches).  Blocks until done.  Replaces the per-step TimeEventUpdateNeurons /
+ * TimeDrivenInternalSpike / PropagatedSpikeGroup cycle. */
+int eb_run(eb_ctx *ctx, int64_t n_steps);
+int eb_set_graph_steps(eb_ctx *ctx, int graph_steps);
+/* Enqueue n_steps on the context stream without synchronizing (error flags are
+ * checked by the next eb_sync / eb_run). */
+int eb_run_async(eb_ctx *ctx, int64_t n_steps);
+int eb_sync(eb_ctx *ctx);
+
+/* -------------------------------------------------------------- outputs --- */
+/* Recording buffer capacity in spikes (default 16M). */
+int eb_set_record_capacity(eb_ctx *ctx, int64_t cap);
+/* Drain recorded spikes (1-based step index, global neuron), sorted by (step, neuron);
+ * the ArrayOutputSpikeDriver::GetBufferedSpikes counterpart
+ * (src/communication/ArrayOutputSpikeDriver.cpp:56-80).  With cap too small, returns
+ * EB_ERR_OVERFLOW and *n the required size without draining. */
+int eb_get_spikes(eb_ctx *ctx, int64_t cap, int64_t *n, int64_t *step, int64_t *cell);
+/* Update time of step k (double seconds, accumulated like the reference). */
+int eb_step_time(eb_ctx *ctx, int64_t k, double *t);
+/* State variable `var` (model order: V first, then the other differential variables,
+ * then gE, gI, gNMDA) of neurons [first, first+n). */
+int eb_get_state(eb_ctx *ctx, int64_t first, int64_t n, int var, float *out);
+int eb_set_state(eb_ctx *ctx, int64_t first, int64_t n, int var, const float *in);
+/* Record all state variables of neurons [first, first+n) after each of the next
+ * `steps` steps: layout [steps][n][8] floats. */
+int eb_set_trace(eb_ctx *ctx, int64_t first, int64_t n, int64_t steps);
+int eb_get_trace(eb_ctx *ctx, float *out);
+/* Weights in network-file order (Network::SaveWeights, src/spike/Network.cpp:1165-1202). */
+int eb_get_weights(eb_ctx *ctx, float *w);
+int eb_set_weights(eb_ctx *ctx, const float *w);
+/* Steps done, spikes emitted, synaptic events delivered. */
+int eb_get_counters(eb_ctx *ctx, int64_t *steps, int64_t *spikes, int64_t *events);
+/* Device memory held by the context, bytes. */
+int eb_device_bytes(eb_ctx *ctx, int64_t *bytes);
+
+/* ---------------------------------------------------- checkpoint/resume --- */
+/* Copy the whole dynamic state (neurons, BDF history, arrival buckets, weights,
+ * plasticity traces, step counter) into an internal snapshot slot / restore it. */
+int eb_snapshot(eb_ctx *ctx, int slot);
+int eb_restore(eb_ctx *ctx, int slot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EDLUT_B200_H */
