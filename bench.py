@@ -1,0 +1,401 @@
+#!/usr/bin/env python3
+"""Benchmark of the time-driven simulation path on B200.
+
+Workload (single-GPU): the cerebellar-layer network -- 250,000 granule-like AdEx
+neurons, each with in-degree 4 from 5,000 Poisson mossy fibres (5-50 Hz uniform),
+plus 200 Purkinje-like LIF neurons each receiving 50,000 granule synapses with
+additive exponential STDP (A+ 1e-3, A- 1.05e-3, tau 20 ms); RK4, dt = 0.1 ms,
+float32; synthetic seeded inputs (no dataset).  One benchmark step = 1,000
+integration steps (100 ms of simulated time) of that network, continuing the
+same simulation.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``value`` is neuron-updates/s with the inputs
+already in HBM (device time, CUDA events on the library's stream, L2 flushed
+between benchmark steps); ``e2e`` is the same metric through the public API with
+the step's input spikes copied in from host memory and its spikes read back.
+``--impl reference`` times the reference EDLUT CPU kernel (built from the
+reference sources into oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "neuron-updates/s"
+UNIT = "neuron-updates/s"
+STEPS_PER_BENCH_STEP = 1000
+DT = 1e-4
+WORKLOAD = "cerebellar-layer: 250k AdEx granule (in-degree 4 from 5k Poisson mossy 5-50 Hz) + 200 LIF Purkinje x 50k plastic granule synapses, STDP A+1e-3 A-1.05e-3 tau 20 ms, RK4 dt 0.1 ms, fp32"
+BYTES_PER_UNIT = {"AdEx": 32, "LIF": 32, "HH": 48}  # algorithmic bytes per neuron-update
+EVENT_BYTES = 8
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
+        if shutil.which("nvidia-smi"):
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_workload(seed: int, t_end: float, scale: float = 1.0):
+    from edlut_b200 import configs
+    n_g = int(250_000 * scale)
+    n_mf = max(1, int(5_000 * scale))
+    n_pc = max(1, int(200 * scale))
+    k = int(50_000 * scale)
+    return configs.cerebellar_layer(seed=seed, n_granule=n_g, n_mossy=n_mf, n_purkinje=n_pc,
+                                    pf_per_purkinje=k, t_end=t_end)
+
+
+# ------------------------------------------------------------- our arm ----
+def run_ours(args):
+    import torch
+    rank, world, local = env_rank()
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    from edlut_b200.simulation import Simulation
+    from edlut_b200 import _lib
+
+    W, K = args.warmup, args.steps
+    prof_steps = 1
+    total_bench = W + K + prof_steps + K  # warmup, timed, profiled, e2e
+    t_total = (total_bench * STEPS_PER_BENCH_STEP + 10) * DT
+    net, tin, cin = build_workload(seed=1 + rank, t_end=t_total, scale=args.scale)
+    n_model = sum(l.n for l in net.layers if l.model != "InputSpikeNeuronModel")
+    sim = Simulation.from_description(net, device=dev, record_capacity=8 << 20)
+    L = _lib.load()
+    import ctypes
+    sp = ctypes.c_void_p()
+    _lib.check(L.eb_stream(sim._h, ctypes.byref(sp)))
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", dev))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    # inputs of warmup + timed + profiled steps resident in HBM before timing
+    n_dev_steps = (W + K + prof_steps) * STEPS_PER_BENCH_STEP
+    t_dev_end = sim.step_time(n_dev_steps)
+    sel = tin < t_dev_end
+    sim.inject_spikes(tin[sel], cin[sel])
+    _lib.check(L.eb_prestage(sim._h, n_dev_steps))
+
+    for _ in range(W):
+        sim.run(STEPS_PER_BENCH_STEP)
+    sim.spikes()
+    c0 = sim.counters()
+    l0 = ctypes.c_int64(0)
+    _lib.check(L.eb_launch_count(sim._h, ctypes.byref(l0)))
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    for i in range(K):
+        with torch.cuda.stream(stream):
+            flush.fill_(i & 0xff)  # evict L2 between benchmark steps (outside the timed events)
+            ev[i][0].record(stream)
+        sim.run_async(STEPS_PER_BENCH_STEP)
+        ev[i][1].record(stream)
+    sim.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    c1 = sim.counters()
+    l1 = ctypes.c_int64(0)
+    _lib.check(L.eb_launch_count(sim._h, ctypes.byref(l1)))
+    sec = ms / 1e3
+    if world > 1:
+        t = torch.tensor([sec], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        sec = float(t.item())
+    updates_rank = n_model * STEPS_PER_BENCH_STEP * K
+    events_rank = c1["events"] - c0["events"]
+    spikes_rank = c1["spikes"] - c0["spikes"]
+    sim.spikes()
+
+    # per-kernel durations: the same steps replayed as a graph with event-record
+    # nodes around every kernel on the stream it runs on
+    _lib.check(L.eb_set_profile(sim._h, 1))
+    for _ in range(prof_steps * STEPS_PER_BENCH_STEP // 250):
+        sim.run(250)
+    n = ctypes.c_int(0)
+    cap = 64
+    kinds = (ctypes.c_int * cap)()
+    popi = (ctypes.c_int * cap)()
+    lau = (ctypes.c_int64 * cap)()
+    tms = (ctypes.c_double * cap)()
+    _lib.check(L.eb_get_profile(sim._h, cap, ctypes.byref(n), kinds, popi, lau, tms))
+    _lib.check(L.eb_set_profile(sim._h, 0))
+    kind_names = {0: "input_push", 1: "update", 2: "post_stdp", 3: "push"}
+    prof = []
+    for i in range(n.value):
+        pname = net.layers[popi[i]].name if popi[i] >= 0 else "-"
+        prof.append(dict(kernel="%s[%s]" % (kind_names[kinds[i]], pname), launches=int(lau[i]),
+                         total_ms=float(tms[i]), avg_us=1e3 * float(tms[i]) / max(1, int(lau[i]))))
+    tot = sum(p["total_ms"] for p in prof) or 1.0
+    for p in prof:
+        p["share"] = p["total_ms"] / tot
+    prof.sort(key=lambda p: -p["total_ms"])
+    sim.spikes()
+
+    # end to end through the public API: host input arrays in, spikes out
+    e2e_s = 0.0
+    h2d = d2h = 0
+    for i in range(K):
+        k_lo = sim.counters()["steps"]
+        t_lo, t_hi = sim.step_time(k_lo), sim.step_time(k_lo + STEPS_PER_BENCH_STEP)
+        m = (tin >= t_lo) & (tin < t_hi)
+        ht = np.ascontiguousarray(tin[m])
+        hc = np.ascontiguousarray(cin[m])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.inject_spikes(ht, hc)
+        sim.run(STEPS_PER_BENCH_STEP)
+        st, ce = sim.spikes()
+        e2e_s += time.perf_counter() - t0
+        h2d += int(m.sum()) * (8 + 4) + (STEPS_PER_BENCH_STEP + 1) * 8
+        d2h += len(st) * 8 + 8
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    # roofline of the dominant kernel
+    peak, peak_kind = measured_peaks()
+    top = prof[0]
+    pop_name = top["kernel"].split("[")[1].rstrip("]")
+    layer = next((l for l in net.layers if l.name == pop_name), None)
+    if top["kernel"].startswith("update") and layer is not None:
+        mdl = "AdEx" if "AdEx" in layer.model else "HH" if "HH" in layer.model else "LIF"
+        alg_bytes = BYTES_PER_UNIT[mdl] * layer.n
+    else:
+        alg_bytes = EVENT_BYTES * events_rank / (STEPS_PER_BENCH_STEP * K)
+    achieved = alg_bytes / (top["avg_us"] * 1e-6) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(top["kernel"])
+
+    # cpu baseline (rank 0 only, N=1): reference CPU kernel on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_sample(args, steps=args.cpu_sample_steps)
+
+    result = {
+        "metric": METRIC, "value": world * updates_rank / sec, "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": 1e3 * sec / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (state), f64 (event times)",
+        "data": "synthetic (seeded Poisson mossy-fibre inputs, random connectivity)",
+        "config": {"workload": WORKLOAD, "integration_steps_per_step": STEPS_PER_BENCH_STEP,
+                   "neurons": n_model, "synapses": int(net.n_synapses), "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed (256 MB write) between timed steps", "scale": args.scale},
+        "syn_events_per_s": world * events_rank / sec,
+        "spikes_per_s": world * spikes_rank / sec,
+        "e2e": {"value": world * updates_rank / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // K,
+                "d2h_bytes_per_step": d2h // K},
+        "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "avg_launch_us": top["avg_us"]},
+        "kernels": prof[:8],
+        "gpu_launches": int(l1.value - l0.value),
+        "clocks": clk,
+        "cpu_baseline": cpu,
+    }
+    sim.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result))
+
+
+# ------------------------------------------------------- reference arm ----
+def ref_binary():
+    p = os.path.join(ROOT, "oracle", "_ref", "EDLUTKernel")
+    return p if os.path.exists(p) else None
+
+
+def cpu_reference_sample(args, steps: int, threads: int | None = None):
+    """Time the reference EDLUT CPU kernel (EDLUTKernel, -openmp Q) on a bounded
+    sample of the workload: the cerebellar layer at 1/10 scale (25k granule AdEx,
+    500 mossy fibres, 20 Purkinje x 5k plastic synapses), `steps` integration steps.
+    Setup is removed by subtracting a 1-step run.  Falls back to the C oracle port
+    (single thread) when the reference build is absent."""
+    scale = 0.1
+    t_end = (steps + 20) * DT
+    net, tin, cin = build_workload(seed=11, t_end=t_end, scale=scale)
+    n_model = sum(l.n for l in net.layers if l.model != "InputSpikeNeuronModel")
+    exe = ref_binary()
+    cores = threads or os.cpu_count() or 1
+    if exe is None:
+        from oracle import oracle as O
+        t0 = time.perf_counter()
+        r = O.run(net, tin, cin, steps)
+        el = time.perf_counter() - t0
+        return {"value": n_model * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": "C oracle port, cerebellar layer at 1/10 scale, %d steps" % steps,
+                "syn_events_per_s": r["n_events"] / el}
+    from edlut_b200.network import write_input_spikes
+    wd = tempfile.mkdtemp(prefix="edlut_ref_")
+    netf, wf = net.write_files(wd)
+    write_input_spikes(os.path.join(wd, "inputs.cfg"), tin, cin)
+
+    def run(nst):
+        cmd = [exe, "-time", repr(nst * DT + 0.5 * DT), "-nf", os.path.basename(netf), "-wf",
+               os.path.basename(wf), "-if", "inputs.cfg", "-openmp", str(cores)]
+        t0 = time.perf_counter()
+        r = subprocess.run(cmd, cwd=wd, capture_output=True, text=True)
+        el = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError("EDLUTKernel failed: " + r.stdout[-500:] + r.stderr[-500:])
+        ev = 0
+        for line in r.stdout.splitlines():
+            if line.startswith("Total Propagated Spikes and Events"):
+                ev = int(line.split(":")[1].split(",")[0])
+        return el, ev
+    t1, _ = run(1)
+    tn, ev = run(steps)
+    shutil.rmtree(wd, ignore_errors=True)
+    sim_s = max(tn - t1, 1e-9)
+    return {"value": n_model * (steps - 1) / sim_s, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": "reference EDLUTKernel -openmp %d, cerebellar layer at 1/10 scale (%d neurons), %d steps, "
+                      "setup removed by subtracting a 1-step run" % (cores, n_model, steps),
+            "syn_events_per_s": ev / sim_s}
+
+
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    samples = []
+    W, K = args.warmup, args.steps
+    for i in range(W + K):
+        r = cpu_reference_sample(args, steps=args.cpu_sample_steps)
+        if i >= W:
+            samples.append(r)
+    v = statistics.mean(s["value"] for s in samples)
+    ev = statistics.mean(s["syn_events_per_s"] for s in samples)
+    result = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": K,
+              "warmup": W, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+              "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+              "config": {"workload": WORKLOAD, "sample": samples[0]["sample"]},
+              "syn_events_per_s": ev,
+              "cpu_baseline": {"value": v, "unit": UNIT, "cores": samples[0]["cores"], "kind": samples[0]["kind"],
+                               "sample": samples[0]["sample"]},
+              "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(result))
+
+
+def run_for_profiler(args):
+    """Build the workload and run it with no timing, for an external profiler:
+    `args.prof_warm` warm-up steps then `args.prof_run` steps, graph replay of
+    `args.graph_steps` steps (1: one launch per kernel, so each is listed)."""
+    from edlut_b200.simulation import Simulation
+    n = args.prof_warm + args.prof_run
+    net, tin, cin = build_workload(1, (n + 20) * DT, args.scale)
+    sim = Simulation.from_description(net, graph_steps=args.graph_steps)
+    sim.inject_spikes(tin, cin)
+    sim.run(args.prof_warm)
+    t0 = time.perf_counter()
+    sim.run(args.prof_run)
+    el = time.perf_counter() - t0
+    print(json.dumps({"profile_run_steps": args.prof_run, "wall_ms_per_step": 1e3 * el / max(1, args.prof_run),
+                      "counters": sim.counters()}))
+    sim.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--cpu-sample-steps", type=int, default=2000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true", help="untimed run for an external profiler")
+    ap.add_argument("--prof-warm", type=int, default=300)
+    ap.add_argument("--prof-run", type=int, default=50)
+    ap.add_argument("--graph-steps", type=int, default=1)
+    args = ap.parse_args()
+    if args.profile_run:
+        run_for_profiler(args)
+        return
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

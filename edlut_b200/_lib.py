@@ -56,6 +56,12 @@ SIGNATURES = [
     ("eb_set_weights", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
     ("eb_get_counters", ctypes.c_int, [ctypes.c_void_p, c_i64p, c_i64p, c_i64p]),
     ("eb_device_bytes", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
+    ("eb_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("eb_prestage", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("eb_set_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("eb_get_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), c_i64p, c_f64p]),
+    ("eb_launch_count", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
     ("eb_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("eb_restore", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
 ]

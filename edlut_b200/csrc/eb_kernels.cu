@@ -24,6 +24,7 @@
 //   arrival after update at equal time: include/simulation/Event.h:37
 //   input-spike delay cascade: src/spike/PropagatedSpike.cpp:60-100
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
 #include "eb_device.cuh"
 #include "eb_kernels.h"
@@ -215,257 +216,201 @@ __global__ void __launch_bounds__(256) k_update_narrow(PopDev P, NetDev N, int r
 }
 
 // ------------------------------------------------------------- wide update --
-// One warp per neuron, for populations whose neurons receive many arrivals per
-// step (e.g. Purkinje-like cells with 10^4-10^5 inputs).  The warp sorts the
-// arrivals (registers up to 32, shared memory up to kWideSmem, global beyond),
-// then per chunk of 32: every lane loads its synapse and applies the STDP pre
-// update in parallel (synapses are independent), and the conductance sums are
-// accumulated in delivery order by lane 0 from shuffled weights.  A chunk that
-// holds the same synapse twice is processed serially.
-constexpr int kWideWarps = 4;
-constexpr int kWideSmem = 512;
-
-__device__ __forceinline__ void warp_sort32(Arrival &v, int lane) {
-    // bitonic sort of one element per lane by (a, spos)
-#pragma unroll
-    for (int size = 2; size <= 32; size <<= 1) {
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            Arrival o;
-            o.a = __shfl_xor_sync(0xffffffffu, v.a, stride);
-            o.spos = __shfl_xor_sync(0xffffffffu, v.spos, stride);
-            o.tpos = __shfl_xor_sync(0xffffffffu, v.tpos, stride);
-            const bool up = ((lane & size) == 0);
-            const bool lower = ((lane & stride) == 0);
-            const bool take_min = (up == lower);
-            const bool o_less = arr_less(o, v);
-            if (take_min ? o_less : arr_less(v, o)) v = o;
-        }
-    }
-}
-
-template <int ND>
-__device__ void fold_chunk(const NetDev &N, const Arrival &mine, bool valid, int cnt, float *x, int lane) {
-    const unsigned full = 0xffffffffu;
-    // duplicate synapses inside the chunk force the serial path
-    const uint32_t key = valid ? mine.tpos : 0xffffffffu - (uint32_t)lane;
-    const unsigned peers = __match_any_sync(full, key);
-    const bool dup = valid && (__popc(peers) > 1);
-    if (__any_sync(full, dup)) {
-        for (int a = 0; a < cnt; ++a) {
-            Arrival r;
-            r.a = __shfl_sync(full, mine.a, a);
-            r.spos = __shfl_sync(full, mine.spos, a);
-            r.tpos = __shfl_sync(full, mine.tpos, a);
-            if (lane == 0) apply_arrival<ND>(N, r, x);
-            __syncwarp();
-        }
-        return;
-    }
-    float w = 0.0f;
-    int ty = 0;
-    if (valid) {
-        const uint32_t tp = mine.tpos;
-        w = N.w[tp];
-        ty = N.stype[tp];
-        const int rl = N.rule[tp];
-        if (rl >= 0) stdp_pre(N, tp, rl, mine.a);
-    }
-    for (int a = 0; a < cnt; ++a) {
-        const float wa = __shfl_sync(full, w, a);
-        const int ta = __shfl_sync(full, ty, a);
-        if (lane == 0) add_conductance<ND>(x, ta, wa);
-    }
-    __syncwarp();
-}
+// One block per neuron, for populations whose neurons receive many arrivals per
+// step (e.g. Purkinje-like cells with 10^4-10^5 inputs).  The block sorts the
+// arrivals in shared memory (bitonic, up to kWideSmem records), every thread
+// fetches the weight of one arrival and applies its STDP pre-synaptic update in
+// parallel (synapses are independent; a synapse that can arrive twice in one step
+// -- only from input neurons -- forces the serial path), and thread 0 adds the
+// weights into the conductances in delivery order, then integrates the neuron.
+constexpr int kWideThreads = 256;
+constexpr int kWideSmem = 1024;
 
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kWideWarps * 32) k_update_wide(PopDev P, NetDev N, int rel) {
+__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel) {
     constexpr int ND = Model<KIND>::ND;
-    __shared__ Arrival sbuf[kWideWarps][kWideSmem];
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    __shared__ Arrival sbuf[kWideSmem];
+    __shared__ float sw[kWideSmem];
+    __shared__ uint8_t sty[kWideSmem];
+    const int tid = threadIdx.x;
     const int64_t k = cur_step(N, rel);
-    const int64_t i = (int64_t)blockIdx.x * kWideWarps + wid;
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
-    if (i >= P.n) return;
-    const int64_t gi = P.first + i;
-    float x[kMaxVars];
-    load_state<KIND>(P, i, x);  // every lane holds a copy; lane 0's is authoritative
+    if (blockIdx.x == 0 && tid == 0) P.spk_count[(k + 1) & 1] = 0;
     const int slot = (int)(k % N.R);
-    uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
-    uint32_t c = *cp;
-    __syncwarp();
-    if (c) {
-        if (lane == 0) *cp = 0;
-        const uint32_t capg = N.cap[gi];
-        if (c > capg) { if (lane == 0) atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
-        Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
-        if (c <= 32) {
-            Arrival v;
-            const bool valid = lane < (int)c;
-            if (valid) v = r[lane];
-            else { v.a = __longlong_as_double(0x7ff0000000000000LL); v.spos = 0xffffffffu; v.tpos = 0; }
-            warp_sort32(v, lane);
-            fold_chunk<ND>(N, v, lane < (int)c, (int)c, x, lane);
-        } else {
-            Arrival *buf = r;
+    for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) {
+        const int64_t gi = P.first + i;
+        uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
+        uint32_t c = *cp;
+        __syncthreads();
+        float x[kMaxVars];
+        if (tid == 0) load_state<KIND>(P, i, x);
+        if (c) {
+            if (tid == 0) *cp = 0;
+            const uint32_t capg = N.cap[gi];
+            if (c > capg) { if (tid == 0) atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
+            Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
             if (c <= (uint32_t)kWideSmem) {
-                buf = sbuf[wid];
                 int n2 = 1;
                 while (n2 < (int)c) n2 <<= 1;
-                for (int a = lane; a < n2; a += 32) {
-                    if (a < (int)c) buf[a] = r[a];
-                    else { buf[a].a = __longlong_as_double(0x7ff0000000000000LL); buf[a].spos = 0xffffffffu; buf[a].tpos = 0; }
+                for (int a = tid; a < n2; a += kWideThreads) {
+                    if (a < (int)c) sbuf[a] = r[a];
+                    else { sbuf[a].a = __longlong_as_double(0x7ff0000000000000LL); sbuf[a].spos = 0xffffffffu; sbuf[a].tpos = 0; }
                 }
-                __syncwarp();
+                __syncthreads();
                 for (int size = 2; size <= n2; size <<= 1)
                     for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                        for (int a = lane; a < n2; a += 32) {
+                        for (int a = tid; a < n2; a += kWideThreads) {
                             const int b = a ^ stride;
                             if (b > a) {
                                 const bool up = ((a & size) == 0);
-                                Arrival ea = buf[a], eb = buf[b];
-                                if (up ? arr_less(eb, ea) : arr_less(ea, eb)) { buf[a] = eb; buf[b] = ea; }
+                                const Arrival ea = sbuf[a], eb = sbuf[b];
+                                if (up ? arr_less(eb, ea) : arr_less(ea, eb)) { sbuf[a] = eb; sbuf[b] = ea; }
                             }
                         }
-                        __syncwarp();
+                        __syncthreads();
                     }
-            } else if (lane == 0) {
+                if (P.may_repeat) {
+                    if (tid == 0)
+                        for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, sbuf[a], x);
+                } else {
+                    for (int a = tid; a < (int)c; a += kWideThreads) {
+                        const Arrival v = sbuf[a];
+                        const uint32_t tp = v.tpos;
+                        sw[a] = N.w[tp];
+                        sty[a] = N.stype[tp];
+                        const int rl = N.rule[tp];
+                        if (rl >= 0) stdp_pre(N, tp, rl, v.a);
+                    }
+                    __syncthreads();
+                    if (tid == 0)
+                        for (uint32_t a = 0; a < c; ++a) add_conductance<ND>(x, sty[a], sw[a]);
+                }
+            } else if (tid == 0) {
                 for (uint32_t a = 1; a < c; ++a) {  // rare: insertion sort in global memory
                     Arrival v = r[a];
                     int b = (int)a - 1;
                     while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
                     r[b + 1] = v;
                 }
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, r[a], x);
             }
-            __syncwarp();
-            for (uint32_t base = 0; base < c; base += 32) {
-                const int cnt = (int)min(32u, c - base);
-                Arrival v;
-                const bool valid = lane < cnt;
-                if (valid) v = buf[base + lane];
-                fold_chunk<ND>(N, v, valid, cnt, x, lane);
-            }
+            if (tid == 0) atomicAdd(N.events, (unsigned long long)c);
         }
-        if (lane == 0) atomicAdd(N.events, (unsigned long long)c);
-    }
-    bool sp = false;
-    if (lane == 0) {
-        sp = advance_neuron<KIND, INTEG>(P, N, i, x);
-        store_state<KIND>(P, i, x);
-        record_trace(P, N, k, gi, x, Model<KIND>::NV);
-        if (sp) {
-            const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
-            if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
-            else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
-            if (N.rec_buf) {
-                const unsigned long long ro = atomicAdd(N.rec_count, 1ull);
-                if (ro < (unsigned long long)N.rec_cap)
-                    N.rec_buf[ro] = ((unsigned long long)k << 32) | (unsigned long long)gi;
-                else atomicOr(N.flags, FLAG_RECORD_OVERFLOW);
+        if (tid == 0) {
+            const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x);
+            store_state<KIND>(P, i, x);
+            record_trace(P, N, k, gi, x, Model<KIND>::NV);
+            if (sp) {
+                const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
+                if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
+                else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
+                if (N.rec_buf) {
+                    const unsigned long long ro = atomicAdd(N.rec_count, 1ull);
+                    if (ro < (unsigned long long)N.rec_cap)
+                        N.rec_buf[ro] = ((unsigned long long)k << 32) | (unsigned long long)gi;
+                    else atomicOr(N.flags, FLAG_RECORD_OVERFLOW);
+                }
             }
         }
     }
-    (void)full;
 }
 
 // ------------------------------------------------------------ spike fan-out --
 // Arrival step of a delivery at time a: the first update time strictly after a.
-__device__ __forceinline__ int64_t arrival_step(const NetDev &N, double a, int64_t k_lo, double dt_s) {
-    int64_t ka = k_lo + (int64_t)((a - N.tstep[k_lo]) / dt_s);
-    if (ka < k_lo) ka = k_lo;
+// `est` is a close guess; two table reads confirm it in the common case.
+__device__ __forceinline__ int64_t arrival_step(const NetDev &N, double a, int64_t k_lo, int64_t est) {
+    int64_t ka = est < k_lo ? k_lo : est;
     while (N.tstep[ka] <= a) ++ka;
     while (ka > k_lo && N.tstep[ka - 1] > a) --ka;
     return ka;
 }
 
+// Reserve a bucket entry of the target for step ka and store the arrival.
+// Loads that do not depend on the reservation are issued before the atomic.
 __device__ __forceinline__ void bucket_put(const NetDev &N, int64_t ka, double a, int64_t o) {
     const uint32_t tg = N.out_tgt[o];
+    const uint32_t tp = N.out_tpos[o];
+    const uint32_t capg = N.cap[tg];
+    const int64_t base = N.cap_base[tg];
     const int slot = (int)(ka % N.R);
     const uint32_t idx = atomicAdd(N.cnt + (int64_t)slot * N.n_neurons + tg, 1u);
-    if (idx < N.cap[tg]) {
+    if (idx < capg) {
         Arrival v;
         v.a = a;
         v.spos = (uint32_t)o;
-        v.tpos = N.out_tpos[o];
-        N.rec[(int64_t)slot * N.cap_total + N.cap_base[tg] + idx] = v;
+        v.tpos = tp;
+        N.rec[(int64_t)slot * N.cap_total + base + idx] = v;
     } else {
         atomicOr(N.flags, FLAG_BUCKET_OVERFLOW);
     }
 }
 
-// Spikes of population P at step k (update time t_k): one warp per spike, the
-// lanes stride over the source's out-synapses (sorted by delay, then target).
-__global__ void __launch_bounds__(256) k_push(PopDev P, NetDev N, int rel, double dt_s) {
+// Spikes of population P at step k (update time t_k): one block per spike, the
+// threads cover the source's out-synapses (sorted by delay, then target).
+__global__ void __launch_bounds__(256) k_push(PopDev P, NetDev N, int rel, double inv_dt) {
     const int64_t k = cur_step(N, rel);
     const uint32_t ns = min(P.spk_count[k & 1], (uint32_t)P.n);
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const double tk = N.tstep[k];
-    for (int64_t s = warp; s < ns; s += nwarps) {
+    for (int64_t s = blockIdx.x; s < ns; s += gridDim.x) {
         const int64_t src = P.first + P.spk[s];
         const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
-        for (int64_t o = o0 + lane; o < o1; o += 32) {
-            const double a = tk + (double)N.out_units[o] * 0.0001;
-            bucket_put(N, arrival_step(N, a, k + 1, dt_s), a, o);
+        for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
+            const double d = (double)N.out_units[o] * 0.0001;
+            const double a = tk + d;
+            bucket_put(N, arrival_step(N, a, k + 1, k + (int64_t)(d * inv_dt)), a, o);
         }
     }
 }
 
-// Input-neuron spikes emitted in [t_{k-1}, t_k): warp per spike.  A source with
-// several distinct delays delivers group j+1 at (a_j - d_j) + d_{j+1}, as the
+// Input-neuron spikes emitted in [t_{k-1}, t_k): one block per spike.  A source
+// with several distinct delays delivers group j+1 at (a_j - d_j) + d_{j+1}, as the
 // reference's PropagatedSpike chain does.
-__global__ void __launch_bounds__(256) k_input_push(NetDev N, int rel, double dt_s) {
+__global__ void __launch_bounds__(256) k_input_push(NetDev N, int rel, double inv_dt) {
     const int64_t k = cur_step(N, rel);
     const int64_t q0 = N.in_start[k], q1 = N.in_start[k + 1];
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t q = q0 + warp; q < q1; q += nwarps) {
+    const double tprev = N.tstep[k - 1];
+    for (int64_t q = q0 + blockIdx.x; q < q1; q += gridDim.x) {
         const int64_t src = N.in_cell[q];
         const double tin = N.in_time[q];
         const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
         const int64_t g0 = N.grp_ptr[src], g1 = N.grp_ptr[src + 1];
-        for (int64_t o = o0 + lane; o < o1; o += 32) {
+        for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
             const uint16_t u = N.out_units[o];
             double a = tin + (double)N.grp_units[g0] * 0.0001;
             for (int64_t g = g0 + 1; g < g1 && N.grp_units[g - 1] != u; ++g)
                 a = a - (double)N.grp_units[g - 1] * 0.0001 + (double)N.grp_units[g] * 0.0001;
-            bucket_put(N, arrival_step(N, a, k, dt_s), a, o);
+            bucket_put(N, arrival_step(N, a, k, k - 1 + (int64_t)((a - tprev) * inv_dt)), a, o);
         }
     }
 }
 
 // Post-synaptic STDP (STDPWeightChange::ApplyPostSynapticSpike) for every spike
-// of population P at step k.  Work items are (spike, chunk of the neuron's
-// plastic input range); threads stride over the chunk.
-__global__ void __launch_bounds__(256) k_post_stdp(PopDev P, NetDev N, int rel, int chunk, int max_chunks) {
+// of population P at step k.  Work items are (spike, chunk of blockDim plastic
+// input synapses of that neuron); one synapse per thread.
+__global__ void __launch_bounds__(256) k_post_stdp(PopDev P, NetDev N, int rel, int max_chunks) {
     const int64_t k = cur_step(N, rel);
     const uint32_t ns = min(P.spk_count[k & 1], (uint32_t)P.n);
     const double tk = N.tstep[k];
-    for (int64_t item = blockIdx.x; item < (int64_t)ns * max_chunks; item += gridDim.x) {
+    const int64_t items = (int64_t)ns * max_chunks;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
         const int64_t s = item / max_chunks, ch = item % max_chunks;
         const int64_t t = P.first + P.spk[s];
-        const int64_t b0 = N.in_ptr[t] + ch * chunk;
-        const int64_t b1 = min(N.plastic_end[t], b0 + chunk);
-        for (int64_t tp = b0 + threadIdx.x; tp < b1; tp += blockDim.x) {
-            const int rl = N.rule[tp];
-            const float *rp = N.rule_par + rl * 6;
-            const float el = (float)(tk - N.last[tp]);
-            float pre = N.pre[tp] * expt_net(N, -el * rp[4]);
-            float post = N.post[tp] * expt_net(N, -el * rp[5]);
-            N.last[tp] = tk;
-            post += 1.0f;
-            float w = N.w[tp];
-            w += rp[0] * pre;
-            const float mw = N.maxw[tp];
-            if (w > mw) w = mw; else if (w < 0.0f) w = 0.0f;
-            N.pre[tp] = pre;
-            N.post[tp] = post;
-            N.w[tp] = w;
-        }
+        const int64_t tp = N.in_ptr[t] + ch * blockDim.x + threadIdx.x;
+        if (tp >= N.plastic_end[t]) continue;
+        const int rl = N.rule[tp];
+        const float *rp = N.rule_par + rl * 6;
+        const double last = N.last[tp];
+        float pre = N.pre[tp], post = N.post[tp], w = N.w[tp];
+        const float mw = N.maxw[tp];
+        const float el = (float)(tk - last);
+        pre *= expt_net(N, -el * rp[4]);
+        post *= expt_net(N, -el * rp[5]);
+        post += 1.0f;
+        w += rp[0] * pre;
+        if (w > mw) w = mw; else if (w < 0.0f) w = 0.0f;
+        N.last[tp] = tk;
+        N.pre[tp] = pre;
+        N.post[tp] = post;
+        N.w[tp] = w;
     }
 }
 
@@ -475,8 +420,8 @@ __global__ void k_advance(int64_t *step, int K) { *step += K; }
 template <int KIND, int INTEG>
 static void launch_update_t(const PopDev &P, const NetDev &N, int rel, cudaStream_t st) {
     if (P.wide) {
-        const int blocks = (int)((P.n + kWideWarps - 1) / kWideWarps);
-        k_update_wide<KIND, INTEG><<<blocks, kWideWarps * 32, 0, st>>>(P, N, rel);
+        const int blocks = (int)std::min<int64_t>(P.n, 148 * 8);
+        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, 0, st>>>(P, N, rel);
     } else {
         const int blocks = (int)((P.n + 255) / 256);
         k_update_narrow<KIND, INTEG><<<blocks, 256, 0, st>>>(P, N, rel);
@@ -503,16 +448,16 @@ void launch_update(const PopDev &P, const NetDev &N, int rel, cudaStream_t st) {
     }
 }
 
-void launch_push(const PopDev &P, const NetDev &N, int rel, double dt_s, int blocks, cudaStream_t st) {
-    k_push<<<blocks, 256, 0, st>>>(P, N, rel, dt_s);
+void launch_push(const PopDev &P, const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st) {
+    k_push<<<blocks, threads, 0, st>>>(P, N, rel, inv_dt);
 }
 
-void launch_input_push(const NetDev &N, int rel, double dt_s, int blocks, cudaStream_t st) {
-    k_input_push<<<blocks, 256, 0, st>>>(N, rel, dt_s);
+void launch_input_push(const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st) {
+    k_input_push<<<blocks, threads, 0, st>>>(N, rel, inv_dt);
 }
 
-void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int chunk, int max_chunks, int blocks, cudaStream_t st) {
-    k_post_stdp<<<blocks, 256, 0, st>>>(P, N, rel, chunk, max_chunks);
+void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks, int blocks, cudaStream_t st) {
+    k_post_stdp<<<blocks, kPostThreads, 0, st>>>(P, N, rel, max_chunks);
 }
 
 void launch_advance(int64_t *step, int K, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(step, K); }

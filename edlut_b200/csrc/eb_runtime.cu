@@ -271,6 +271,18 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
     has_inputs = false;
     for (auto &p : pops)
         if (p.kind == KIND_INPUT) has_inputs = true;
+    // input fan-out may run beside the neuron updates when no input delivery can
+    // reach the step being updated: every input synapse delay exceeds the step
+    {
+        int64_t min_units = INT64_MAX, max_out_in = 0;
+        for (int64_t i = 0; i < n_neurons; ++i) {
+            if (pops[pop_of[i]].kind != KIND_INPUT) continue;
+            max_out_in = std::max(max_out_in, out_ptr[i + 1] - out_ptr[i]);
+            for (int64_t s = out_ptr[i]; s < out_ptr[i + 1]; ++s) min_units = std::min<int64_t>(min_units, h_out_units[s]);
+        }
+        inputs_concurrent = min_units == INT64_MAX || (double)min_units * 0.0001 > dt_s;
+        input_threads = (int)std::min<int64_t>(256, std::max<int64_t>(32, (max_out_in + 31) / 32 * 32));
+    }
     net = N;
 
     // populations
@@ -358,10 +370,16 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         }
         D.wide = maxcap > 16 ? 1 : 0;
         p.has_plastic_in = max_plastic > 0;
-        p.post_chunks = (int)((max_plastic + kPostChunk - 1) / kPostChunk);
+        p.post_chunks = (int)((max_plastic + kPostThreads - 1) / kPostThreads);
         p.has_out = false;
-        for (int64_t i = p.first; i < p.first + p.n; ++i)
-            if (out_ptr[i + 1] > out_ptr[i]) { p.has_out = true; break; }
+        int64_t max_out = 0, in_from_inputs = 0;
+        for (int64_t i = p.first; i < p.first + p.n; ++i) {
+            if (out_ptr[i + 1] > out_ptr[i]) p.has_out = true;
+            max_out = std::max(max_out, out_ptr[i + 1] - out_ptr[i]);
+            in_from_inputs += indeg_in[i];
+        }
+        p.push_threads = (int)std::min<int64_t>(256, std::max<int64_t>(32, (max_out + 31) / 32 * 32));
+        D.may_repeat = in_from_inputs > 0 ? 1 : 0;
     }
     // dynamic state copied by eb_snapshot / eb_restore
     dyn.clear();
@@ -385,6 +403,18 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
             dyn.push_back({p.dev.bdf_P, sizeof(float) * (size_t)std::max(p.bdf_order - 1, 1) * nd * p.n});
         }
         dyn.push_back({p.dev.spk_count, 2 * sizeof(uint32_t)});
+    }
+    for (int q = 0; q < 4; ++q) {
+        cudaStream_t ss;
+        CK(cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking));
+        side.push_back(ss);
+    }
+    for (int q = 0; q < 8; ++q) {
+        cudaEvent_t a, b;
+        CK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+        fork_ev.push_back(a);
+        join_ev.push_back(b);
     }
     CK(cudaStreamSynchronize(st));
     finalized = true;
@@ -432,6 +462,7 @@ int eb_ctx::ensure_tables(int64_t kmax) {
 // Move pending input spikes with time < t_{k_end} to the device and fill the
 // input ranges of steps k0+1 .. k_end+1.
 int eb_ctx::stage_inputs(int64_t k0, int64_t k_end) {
+    if (k_end <= staged_until && pending.empty()) return EB_OK;
     const double tend = t_host[k_end];
     std::vector<double> nt;
     std::vector<uint32_t> nc;
@@ -473,27 +504,124 @@ int eb_ctx::stage_inputs(int64_t k0, int64_t k_end) {
     CK(cudaMemcpyAsync(d_instart + k0 + 1, h.data(), sizeof(int64_t) * h.size(), cudaMemcpyHostToDevice, stream));
     net.in_time = d_in_time;
     net.in_cell = d_in_cell;
+    staged_until = std::max(staged_until, k_end);
     return EB_OK;
 }
 
+// Profiling: the steps are captured into a graph whose kernels are bracketed
+// by event-record nodes on the stream (branch) each kernel runs on, so the GPU
+// timestamps every launch without the host in the loop.
+void eb_ctx::prof_begin(int kind, int pop, cudaEvent_t *a) {
+    (void)kind; (void)pop;
+    if (!profile) return;
+    if (ev_pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ev_pool.push_back(e);
+    }
+    *a = ev_pool.back();
+    ev_pool.pop_back();
+    cudaEventRecordWithFlags(*a, prof_stream, cudaEventRecordExternal);
+}
+
+void eb_ctx::prof_end(int kind, int pop, cudaEvent_t a) {
+    if (!profile) return;
+    if (ev_pool.empty()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        ev_pool.push_back(e);
+    }
+    cudaEvent_t b = ev_pool.back();
+    ev_pool.pop_back();
+    cudaEventRecordWithFlags(b, prof_stream, cudaEventRecordExternal);
+    prof_pending.push_back({kind, pop, a, b});
+}
+
+int eb_ctx::prof_collect() {
+    for (auto &r : prof_pending) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, r.a, r.b));
+        bool found = false;
+        for (auto &s : prof_sum)
+            if (s.kind == r.kind && s.pop == r.pop) { s.launches++; s.ms += ms; found = true; }
+        if (!found) prof_sum.push_back({r.kind, r.pop, 1, (double)ms});
+        ev_pool.push_back(r.a);
+        ev_pool.push_back(r.b);
+    }
+    prof_pending.clear();
+    return EB_OK;
+}
+
+// Run the launches of one phase on parallel branches (main stream + side
+// streams, joined back into the main stream); sequential when profiling.
+void eb_ctx::fork_join(std::vector<std::function<void(cudaStream_t)>> &work) {
+    if (work.empty()) return;
+    if (work.size() == 1) {
+        for (auto &f : work) f(stream);
+        return;
+    }
+    const size_t nb = std::min(work.size(), side.size() + 1);
+    cudaEventRecord(fork_ev[0], stream);
+    for (size_t b = 1; b < nb; ++b) cudaStreamWaitEvent(side[b - 1], fork_ev[0], 0);
+    for (size_t i = 0; i < work.size(); ++i) {
+        const size_t b = i % nb;
+        work[i](b == 0 ? stream : side[b - 1]);
+    }
+    for (size_t b = 1; b < nb; ++b) {
+        cudaEventRecord(join_ev[b], side[b - 1]);
+        cudaStreamWaitEvent(stream, join_ev[b], 0);
+    }
+}
+
 void eb_ctx::enqueue_step(int rel) {
-    const int fan_blocks = 148 * 2;
-    if (has_inputs) launch_input_push(net, rel, dt_s, fan_blocks, stream);
-    for (auto &p : pops)
-        if (p.kind != KIND_INPUT) launch_update(p.dev, net, rel, stream);
-    for (auto &p : pops) {
+    const int fan_blocks = 148 * 4;
+    const double inv_dt = 1.0 / dt_s;
+    std::vector<std::function<void(cudaStream_t)>> phase;
+    auto timed = [this](int kind, int pop, std::function<void(cudaStream_t)> f) {
+        return [this, kind, pop, f](cudaStream_t s) {
+            cudaEvent_t a = nullptr;
+            prof_stream = s;
+            prof_begin(kind, pop, &a);
+            enq_count++;
+            f(s);
+            prof_end(kind, pop, a);
+        };
+    };
+    if (has_inputs) {
+        auto f = timed(0, -1, [this, rel, inv_dt, fan_blocks](cudaStream_t s) {
+            launch_input_push(net, rel, inv_dt, fan_blocks, input_threads, s);
+        });
+        if (inputs_concurrent) phase.push_back(f);
+        else f(stream);
+    }
+    for (size_t q = 0; q < pops.size(); ++q) {
+        if (pops[q].kind == KIND_INPUT) continue;
+        phase.push_back(timed(1, (int)q, [this, q, rel](cudaStream_t s) { launch_update(pops[q].dev, net, rel, s); }));
+    }
+    fork_join(phase);
+    phase.clear();
+    for (size_t q = 0; q < pops.size(); ++q) {
+        auto &p = pops[q];
         if (p.kind == KIND_INPUT) continue;
         if (p.has_plastic_in)
-            launch_post_stdp(p.dev, net, rel, kPostChunk, p.post_chunks, fan_blocks, stream);
-        if (p.has_out) launch_push(p.dev, net, rel, dt_s, fan_blocks, stream);
+            phase.push_back(timed(2, (int)q, [this, q, rel, fan_blocks](cudaStream_t s) {
+                launch_post_stdp(pops[q].dev, net, rel, pops[q].post_chunks, fan_blocks, s);
+            }));
+        if (p.has_out)
+            phase.push_back(timed(3, (int)q, [this, q, rel, inv_dt, fan_blocks](cudaStream_t s) {
+                launch_push(pops[q].dev, net, rel, inv_dt, fan_blocks, pops[q].push_threads, s);
+            }));
     }
+    fork_join(phase);
 }
 
 int eb_ctx::build_graph(int K) {
     if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    enq_count = 0;
     for (int r = 0; r < K; ++r) enqueue_step(r);
+    graph_kernels = enq_count + 1;
     launch_advance(d_step, K, stream);
     CK(cudaStreamEndCapture(stream, &g));
     cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
@@ -518,17 +646,39 @@ int eb_ctx::run_async(int64_t n) {
     }
     int K = graph_steps > 0 ? graph_steps : 64;
     int64_t done = 0;
+    if (profile) {
+        // one graph of all n steps with timestamped kernels (events are reused only
+        // after prof_collect, so n bounds the number of events in flight)
+        cudaGraph_t g;
+        cudaGraphExec_t ge;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        enq_count = 0;
+        for (int64_t r = 0; r < n; ++r) enqueue_step((int)r);
+        launch_advance(d_step, (int)n, stream);
+        CK(cudaStreamEndCapture(stream, &g));
+        CK(cudaGraphInstantiate(&ge, g, 0));
+        cudaGraphDestroy(g);
+        CK(cudaGraphLaunch(ge, stream));
+        CK(cudaStreamSynchronize(stream));
+        cudaGraphExecDestroy(ge);
+        launches += enq_count + 1;
+        steps_done = k_end;
+        return EB_OK;
+    }
     if (K > 1 && n >= K) {
         if (!graphs_valid || graph_K != K)
             if ((rc = build_graph(K))) return rc;
         while (n - done >= K) {
             CK(cudaGraphLaunch(graph_exec, stream));
+            launches += graph_kernels;
             done += K;
         }
     }
     while (done < n) {
+        enq_count = 0;
         enqueue_step(0);
         launch_advance(d_step, 1, stream);
+        launches += enq_count + 1;
         done++;
     }
     CK(cudaGetLastError());
@@ -538,6 +688,10 @@ int eb_ctx::run_async(int64_t n) {
 
 int eb_ctx::sync() {
     CK(cudaStreamSynchronize(stream));
+    if (profile) {
+        int rc = prof_collect();
+        if (rc) return rc;
+    }
     uint32_t f = 0;
     CK(cudaMemcpy(&f, net.flags, sizeof(f), cudaMemcpyDeviceToHost));
     if (f) {
@@ -595,6 +749,11 @@ int eb_ctx::restore(int slot) {
 
 eb_ctx::~eb_ctx() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto s : side) cudaStreamDestroy(s);
+    for (auto e : fork_ev) cudaEventDestroy(e);
+    for (auto e : join_ev) cudaEventDestroy(e);
+    for (auto &r : prof_pending) { ev_pool.push_back(r.a); ev_pool.push_back(r.b); }
+    for (auto e : ev_pool) cudaEventDestroy(e);
     dfree_all();
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -690,7 +849,14 @@ int eb_inject_spikes(eb_ctx *ctx, int64_t n, const float *time_s, const int64_t 
             return EB_ERR_ARG;
         }
     }
-    for (int64_t i = 0; i < n; ++i) ctx->pending.push_back({time_s[i], cell[i], ctx->pending_seq++});
+    for (int64_t i = 0; i < n; ++i) {
+        ctx->pending.push_back({time_s[i], cell[i], ctx->pending_seq++});
+        // a model neuron used as an input source can deliver twice in one step
+        if (ctx->finalized && ctx->pops[ctx->pop_of[cell[i]]].kind != KIND_INPUT) {
+            for (auto &p : ctx->pops) p.dev.may_repeat = 1;
+            ctx->graphs_valid = false;
+        }
+    }
     std::stable_sort(ctx->pending.begin(), ctx->pending.end(), [](const PendingIn &a, const PendingIn &b) {
         if (a.t != b.t) return a.t < b.t;
         return a.seq < b.seq;
@@ -858,6 +1024,53 @@ int eb_snapshot(eb_ctx *ctx, int slot) {
 int eb_restore(eb_ctx *ctx, int slot) {
     if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
     return ctx->restore(slot);
+}
+
+int eb_stream(eb_ctx *ctx, void **stream) {
+    if (!ctx || !stream) { set_error("bad argument"); return EB_ERR_ARG; }
+    *stream = (void *)ctx->stream;
+    return EB_OK;
+}
+
+int eb_prestage(eb_ctx *ctx, int64_t n_steps) {
+    if (!ctx || n_steps < 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    CK(cudaSetDevice(ctx->device));
+    const int64_t k0 = ctx->steps_done, k_end = k0 + n_steps;
+    int rc;
+    if ((rc = ctx->ensure_tables(k_end + ctx->R + 8))) return rc;
+    if ((rc = ctx->stage_inputs(k0, k_end))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return EB_OK;
+}
+
+int eb_set_profile(eb_ctx *ctx, int on) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    ctx->profile = on != 0;
+    ctx->prof_sum.clear();
+    return EB_OK;
+}
+
+int eb_get_profile(eb_ctx *ctx, int cap, int *n, int *kind, int *pop, int64_t *launches, double *total_ms) {
+    if (!ctx || !n) { set_error("bad argument"); return EB_ERR_ARG; }
+    int c = 0;
+    for (auto &s : ctx->prof_sum) {
+        if (c < cap) {
+            if (kind) kind[c] = s.kind;
+            if (pop) pop[c] = s.pop;
+            if (launches) launches[c] = s.launches;
+            if (total_ms) total_ms[c] = s.ms;
+        }
+        c++;
+    }
+    *n = c;
+    return EB_OK;
+}
+
+int eb_launch_count(eb_ctx *ctx, int64_t *launches) {
+    if (!ctx || !launches) { set_error("bad argument"); return EB_ERR_ARG; }
+    *launches = ctx->launches;
+    return EB_OK;
 }
 
 int eb_device_bytes(eb_ctx *ctx, int64_t *bytes) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <array>
+#include <functional>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -13,7 +14,7 @@ namespace eb {
 
 void set_error(const char *fmt, ...);
 
-constexpr int kPostChunk = 2048;  // plastic synapses per post-STDP work item
+
 
 struct HostPop {
     int kind = KIND_INPUT, integ = 0, bdf_order = 0;
@@ -23,6 +24,7 @@ struct HostPop {
     int en = 0;                 // enabled conductance types (from the synapse types targeting it)
     bool has_out = false, has_plastic_in = false;
     int post_chunks = 1;
+    int push_threads = 32;
     PopDev dev{};
 };
 
@@ -58,6 +60,11 @@ struct eb_ctx {
     int64_t *d_step = nullptr;
     float *d_w = nullptr;
     bool has_inputs = false;
+    bool inputs_concurrent = false;  // input fan-out can overlap the neuron updates
+    int input_threads = 32;
+    // side streams and events for the parallel branches of a step
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> fork_ev, join_ev;
     // time grid and inputs
     std::vector<double> t_host;
     double *d_tstep = nullptr;
@@ -80,6 +87,17 @@ struct eb_ctx {
     bool graphs_valid = false;
     bool trace_pending = false;
     size_t trace_bytes = 0;
+    int64_t staged_until = 0;
+    int64_t launches = 0;          // kernels launched (graph nodes counted per replay)
+    int enq_count = 0, graph_kernels = 0;      // input ranges valid for steps <= staged_until
+    // per-kernel profiling (plain launches with CUDA events around each kernel)
+    bool profile = false;
+    cudaStream_t prof_stream = nullptr;
+    struct ProfRec { int kind, pop; cudaEvent_t a, b; };
+    std::vector<ProfRec> prof_pending;
+    struct ProfSum { int kind, pop; int64_t launches; double ms; };
+    std::vector<ProfSum> prof_sum;
+    std::vector<cudaEvent_t> ev_pool;
     // allocations
     std::vector<void *> allocs;
     int64_t dev_bytes = 0;
@@ -97,6 +115,10 @@ struct eb_ctx {
     int ensure_tables(int64_t kmax);
     int stage_inputs(int64_t k0, int64_t k_end);
     void enqueue_step(int rel);
+    void fork_join(std::vector<std::function<void(cudaStream_t)>> &work);
+    void prof_begin(int kind, int pop, cudaEvent_t *a);
+    void prof_end(int kind, int pop, cudaEvent_t a);
+    int prof_collect();
     int build_graph(int K);
     int run_async(int64_t n);
     int sync();

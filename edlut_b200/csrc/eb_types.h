@@ -53,7 +53,8 @@ struct PopDev {
     uint32_t *spk;
     uint32_t *spk_count;  // [2]
     // in-synapse ranges (target-major) for neurons of this population
-    int wide;            // 1: warp-per-neuron update (large in-degree)
+    int wide;            // 1: block-per-neuron update (large in-degree)
+    int may_repeat;      // a synapse may deliver twice in one step (input-neuron sources)
 };
 
 // Network-wide device pointers, passed by value to the kernels.

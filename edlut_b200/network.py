@@ -193,25 +193,44 @@ def write_input_spikes(path: str, times: Sequence[float], cells: Sequence[int]) 
 
 
 def poisson_input_times(rng: np.random.Generator, n_inputs: int, rate_hz, t_end: float,
-                        dt: float = 1e-4) -> tuple:
+                        dt: float = 1e-4, t_start: float = 0.0) -> tuple:
     """Seeded Poisson spike lists for ``n_inputs`` input neurons, as (times, cells).
 
-    Times are float32 and placed strictly inside a step window (10%..90% of the way
-    between two update times) so that no input event coincides with a neuron update;
-    each time is unique, so the reference's event order at equal time stamps never
-    matters.  Times are sorted.
+    Each input spikes in a step of length ``dt`` with probability rate*dt (at most
+    once per step), drawn as geometric gaps between spike steps.  Times are float32
+    and placed strictly inside a step window (10%..90% of the way between two update
+    times) so that no input event coincides with a neuron update; every time is
+    unique, so the reference's order of events at equal time stamps never matters.
+    Sorted by time.
     """
     rate = np.broadcast_to(np.asarray(rate_hz, np.float64), (n_inputs,))
-    nsteps = int(round(t_end / dt))
-    p = rate * dt
-    hits = rng.random((nsteps, n_inputs)) < p[None, :]
-    step, cell = np.nonzero(hits)
+    k0 = int(round(t_start / dt))
+    nsteps = int(round(t_end / dt)) - k0
+    p = np.clip(rate * dt, 0.0, 1.0)
+    mean = p * nsteps
+    cap = int(np.max(mean + 8.0 * np.sqrt(mean + 1.0) + 8.0)) if n_inputs else 0
+    steps_all, cells_all = [], []
+    for lo in range(0, n_inputs, 4096):
+        hi = min(n_inputs, lo + 4096)
+        pp = np.maximum(p[lo:hi], 1e-300)
+        gaps = rng.geometric(pp[:, None], size=(hi - lo, cap))
+        st = np.cumsum(gaps, axis=1) - 1
+        ok = st < nsteps
+        ok &= (p[lo:hi] > 0)[:, None]
+        r, c = np.nonzero(ok)
+        steps_all.append(st[r, c] + k0)
+        cells_all.append(r + lo)
+    step = np.concatenate(steps_all) if steps_all else np.zeros(0, np.int64)
+    cell = np.concatenate(cells_all) if cells_all else np.zeros(0, np.int64)
     frac = 0.1 + 0.8 * rng.random(len(step))
     times = ((step + frac) * dt).astype(np.float32)
-    # make float32 times unique (nudge collisions by one ulp)
     order = np.lexsort((cell, times))
     times, cell = times[order], cell[order]
-    for i in range(1, len(times)):
-        if times[i] <= times[i - 1]:
-            times[i] = np.nextafter(times[i - 1], np.float32(np.inf))
+    # make float32 times unique (nudge collisions up by one ulp)
+    dup = np.nonzero(times[1:] <= times[:-1])[0]
+    while len(dup):
+        for i in dup + 1:
+            if times[i] <= times[i - 1]:
+                times[i] = np.nextafter(times[i - 1], np.float32(np.inf))
+        dup = np.nonzero(times[1:] <= times[:-1])[0]
     return times, cell.astype(np.int64)

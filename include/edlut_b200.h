@@ -10,17 +10,13 @@
  * References are paths in the EDLUT reference tree, relative to its Kernel/
  * directory.
  *
- * Two levels:
- *  1. Network level (device-resident network): populations, synapses, STDP rules,
+ * Device-resident network: populations, synapses, STDP rules,
  *     input spikes and K-step runs all on the GPU.  Replaces the per-step host work
  *     of the reference engine for time-driven networks: TimeEventUpdateNeurons
  *     (src/simulation/TimeEventUpdateNeurons.cpp:82-116), TimeDrivenInternalSpike
  *     (src/spike/TimeDrivenInternalSpike.cpp:182-253), PropagatedSpikeGroup delivery
  *     (src/spike/PropagatedSpikeGroup.cpp:112-149) and the STDP hooks
  *     (src/learning_rules/STDPWeightChange.cpp:43-76).
- *  2. Model level (eb_model_*): one time-driven neuron population stepped by a host
- *     engine, the drop-in for TimeDrivenNeuronModel_GPU_C_INTERFACE
- *     (include/neuron_model/TimeDrivenNeuronModel_GPU_C_INTERFACE.cuh:64-423).
  */
 #ifndef EDLUT_B200_H
 #define EDLUT_B200_H
@@ -148,6 +144,21 @@ int eb_set_weights(eb_ctx *ctx, const float *w);
 int eb_get_counters(eb_ctx *ctx, int64_t *steps, int64_t *spikes, int64_t *events);
 /* Device memory held by the context, bytes. */
 int eb_device_bytes(eb_ctx *ctx, int64_t *bytes);
+
+/* The context's CUDA stream (cudaStream_t as a pointer), for callers that order
+ * their own work or CUDA events against the simulation. */
+int eb_stream(eb_ctx *ctx, void **stream);
+/* Move the input spikes and step tables of the next n_steps to the device now, so
+ * a following eb_run of those steps does no host-to-device copy. */
+int eb_prestage(eb_ctx *ctx, int64_t n_steps);
+/* Per-kernel timing: with on != 0, runs use plain launches with CUDA events around
+ * every kernel; eb_get_profile returns, per (kernel kind, population), the launch
+ * count and total milliseconds.  kind: 0 input fan-out, 1 neuron update,
+ * 2 post-synaptic STDP, 3 spike fan-out; pop: population index (-1: none). */
+int eb_set_profile(eb_ctx *ctx, int on);
+int eb_get_profile(eb_ctx *ctx, int cap, int *n, int *kind, int *pop, int64_t *launches, double *total_ms);
+/* Number of library kernels launched so far (nodes of a replayed graph counted per replay). */
+int eb_launch_count(eb_ctx *ctx, int64_t *launches);
 
 /* ---------------------------------------------------- checkpoint/resume --- */
 /* Copy the whole dynamic state (neurons, BDF history, arrival buckets, weights,

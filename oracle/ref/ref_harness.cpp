@@ -17,7 +17,8 @@
 //
 // The step loop mirrors EDLUTKernel's RunSimulation by slots: RunSimulationSlot
 // (Simulation.cpp:322) is called with a preempt time half a tenth of a step
-// after each update time, so the event order inside a step is the reference's.
+// after each update time (just after the last one), so the event order inside a
+// step is the reference's.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -80,7 +81,9 @@ int main(int argc, char **argv) {
         double t = 0.0;
         for (long k = 1; k <= nsteps; ++k) {
             t += (double)dt;  // the update event re-arms at CurrentTime + step (TimeEventUpdateNeurons.cpp:115)
-            sim.RunSimulationSlot(t + 0.05 * (double)dt);
+            // after the last update stop before any later delivery (arrivals trail an
+            // update time by at least ~1e-12 s), so final weights carry no partial step
+            sim.RunSimulationSlot(k == nsteps ? t + 1e-13 : t + 0.05 * (double)dt);
             if (ft && k <= trace_steps) {
                 for (long c = trace_first; c < trace_first + trace_n; ++c) {
                     Neuron *n = nw->GetNeuronAt(c);

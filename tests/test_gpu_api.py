@@ -1,0 +1,210 @@
+"""GPU tests of the C-ABI behaviour around the hot path: graph replay vs plain
+launches, chunked runs, snapshot/restore, the reference-format file readers,
+error paths that leave the context usable, determinism, and size-independent
+properties of a benchmark-size run."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests._cases import build_case, spike_pairs
+
+pytestmark = pytest.mark.gpu
+
+
+def make_sim(net, **kw):
+    from edlut_b200.simulation import Simulation
+    return Simulation.from_description(net, **kw)
+
+
+def run_case(name, chunks=None, **kw):
+    net, t, c, nsteps, trace = build_case(name)
+    sim = make_sim(net, **kw)
+    sim.inject_spikes(t, c)
+    for n in (chunks or [nsteps]):
+        sim.run(n)
+    st, ce = sim.spikes()
+    w = sim.weights()
+    sim.close()
+    return spike_pairs(st, ce), w
+
+
+def test_graph_and_plain_launches_agree():
+    a, wa = run_case("adex_rk4_stdp", graph_steps=64)
+    b, wb = run_case("adex_rk4_stdp", graph_steps=1)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(wa, wb)
+
+
+def test_chunked_runs_agree():
+    a, wa = run_case("lif_bdf2_stdp")
+    b, wb = run_case("lif_bdf2_stdp", chunks=[1, 63, 64, 500, 372, 1000])
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(wa, wb)
+
+
+def test_runs_are_deterministic():
+    a, wa = run_case("cereb_small_rk4")
+    b, wb = run_case("cereb_small_rk4")
+    np.testing.assert_array_equal(a, b)
+    assert wa.tobytes() == wb.tobytes()
+
+
+def test_snapshot_restore_replays_identically():
+    net, t, c, nsteps, _ = build_case("hh_bdf2_stdp")
+    sim = make_sim(net)
+    sim.inject_spikes(t, c)
+    sim.run(700)
+    sim.spikes()
+    sim.snapshot(0)
+    sim.run(600)
+    s1 = spike_pairs(*sim.spikes())
+    w1 = sim.weights()
+    sim.restore(0)
+    sim.run(600)
+    s2 = spike_pairs(*sim.spikes())
+    w2 = sim.weights()
+    sim.close()
+    np.testing.assert_array_equal(s1, s2)
+    np.testing.assert_array_equal(w1, w2)
+
+
+def test_reference_files_load_identically(tmp_path):
+    """eb_load_network_files / eb_load_input_file read the reference's own text
+    formats (network, weights, model .cfg, input spikes) into the same network."""
+    from edlut_b200.network import write_input_spikes
+    from edlut_b200.simulation import Simulation
+    net, t, c, nsteps, _ = build_case("lif_rk2_stdp")
+    netf, wf = net.write_files(str(tmp_path))
+    inp = os.path.join(str(tmp_path), "inputs.cfg")
+    write_input_spikes(inp, t, c)
+    cwd = os.getcwd()
+    os.chdir(str(tmp_path))
+    try:
+        sim = Simulation.from_files(os.path.basename(netf), os.path.basename(wf))
+        sim.n_synapses = net.n_synapses
+        sim.load_input_file("inputs.cfg")
+        sim.run(nsteps)
+        a = spike_pairs(*sim.spikes())
+        wa = sim.weights()
+        sim.close()
+    finally:
+        os.chdir(cwd)
+    b, wb = run_case("lif_rk2_stdp")
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(wa, wb)
+
+
+def test_random_weights_follow_reference_lcg(tmp_path, oracle):
+    """A negative weight in the weights file draws uniform [0, max_weight] weights
+    from the reference's LCG (seed 1), in file order."""
+    from edlut_b200.simulation import Simulation
+    net, t, c, nsteps, _ = build_case("lif_euler_stdp")
+    netf, wf = net.write_files(str(tmp_path))
+    with open(wf, "w") as f:
+        f.write("0 -1\n")  # all synapses random
+    cwd = os.getcwd()
+    os.chdir(str(tmp_path))
+    try:
+        sim = Simulation.from_files(os.path.basename(netf), os.path.basename(wf))
+        sim.n_synapses = net.n_synapses
+        w = sim.weights()
+        sim.close()
+    finally:
+        os.chdir(cwd)
+    # restate the LCG here: next = (next*1103515245 + 12345) & 0x7fffffff, first state 1
+    nxt = 1
+    exp = np.zeros(net.n_synapses, np.float32)
+    for i in range(net.n_synapses):
+        nxt = (nxt * 1103515245 + 12345) & 0x7FFFFFFF
+        exp[i] = np.float32(np.float32(nxt) / np.float32(2147483647)) * net.max_weight[i]
+    np.testing.assert_array_equal(w, exp)
+
+
+def test_bucket_overflow_is_reported_and_context_survives():
+    from edlut_b200._lib import EdlutError
+    net, t, c, nsteps, _ = build_case("adex_dense_fanin")
+    sim = make_sim(net, bucket_limit=1)
+    sim.inject_spikes(t, c)
+    with pytest.raises(EdlutError) as e:
+        sim.run(500)
+    assert e.value.code == -4
+    # the context stays usable: state, counters and snapshots still work
+    v = sim.get_state(net.layers[0].n, 10)
+    assert np.all(np.isfinite(v))
+    assert sim.counters()["steps"] == 500
+    sim.snapshot(0)
+    sim.restore(0)
+    sim.close()
+
+
+def test_bad_calls_return_errors():
+    from edlut_b200._lib import EdlutError
+    from edlut_b200.simulation import Simulation
+    sim = Simulation()
+    with pytest.raises(EdlutError):
+        sim.run(10)  # not finalized
+    from edlut_b200.network import MODEL_DEFAULTS
+    sim.add_population("LIFTimeDrivenModel", 10, "Euler", 1, 1e-4, MODEL_DEFAULTS["LIFTimeDrivenModel"])
+    sim.finalize()
+    with pytest.raises(EdlutError):  # populations cannot be added after finalize
+        sim.add_population("LIFTimeDrivenModel", 10, "Euler", 1, 1e-4, MODEL_DEFAULTS["LIFTimeDrivenModel"])
+    from edlut_b200.simulation import Simulation as S2
+    s2 = S2()
+    assert s2._L.eb_add_population(s2._h, 1, 10, 9, 1, 1e-4, None, 0, None) == -6  # unknown integrator
+    assert s2._L.eb_add_population(s2._h, 1, 0, 0, 1, 1e-4, None, 0, None) == -1   # empty population
+    s2.close()
+    sim.close()
+
+
+def test_input_before_current_time_rejected():
+    from edlut_b200._lib import EdlutError
+    net, t, c, nsteps, _ = build_case("lif_euler_stdp")
+    sim = make_sim(net)
+    sim.run(100)
+    with pytest.raises(EdlutError):
+        sim.inject_spikes([0.001], [0])
+    sim.close()
+
+
+def test_empty_connectivity_matches_oracle(oracle):
+    from edlut_b200.network import Layer, NetworkDescription
+    from edlut_b200.configs import LIF_C1
+    net = NetworkDescription()
+    net.add_layer(Layer(100, "LIFTimeDrivenModel", dict(LIF_C1, e_leak=-40.0), integrator="RK4"))
+    sim = make_sim(net)
+    sim.set_trace(0, 4, 50)
+    sim.run(200)
+    tr = sim.get_trace()
+    st, ce = sim.spikes()
+    o = oracle.run(net, np.zeros(0, np.float32), np.zeros(0, np.int64), 200, trace=(50, 0, 4),
+                   spike_cap=100 * 200 + 16)
+    np.testing.assert_array_equal(spike_pairs(st, ce), spike_pairs(o["spike_step"], o["spike_cell"]))
+    np.testing.assert_array_equal(tr, o["trace"].astype(np.float32))
+    sim.close()
+
+
+@pytest.mark.slow
+def test_benchmark_size_properties():
+    """Full cerebellar-layer network (11M synapses): size-independent checks --
+    spikes recorded for both layers, plastic weights within [0, max], no overflow,
+    and two runs from the same seed give byte-identical weights."""
+    import bench
+    net, t, c = bench.build_workload(seed=1, t_end=0.06)
+    outs = []
+    for _ in range(2):
+        sim = make_sim(net)
+        sim.inject_spikes(t, c)
+        sim.run(500)
+        st, ce = sim.spikes()
+        w = sim.weights()
+        outs.append((st, ce, w))
+        sim.close()
+    st, ce, w = outs[0]
+    n_mf, n_g = net.layers[0].n, net.layers[1].n
+    assert ((ce >= n_mf) & (ce < n_mf + n_g)).sum() > 0
+    plastic = net.wchange >= 0
+    assert np.all(w[plastic] >= 0) and np.all(w[plastic] <= net.max_weight[plastic])
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    assert outs[0][2].tobytes() == outs[1][2].tobytes()

@@ -1,0 +1,42 @@
+"""The CPU oracle reproduces the reference's own outputs (golden fixtures made by
+running the reference EDLUT CPU kernel, tests/golden/make_golden.py) bit for bit:
+spike steps and cells, state traces, final STDP weights, synapse order, counts."""
+import numpy as np
+import pytest
+
+from tests._cases import CASES, build_case, load_golden, perm_digest, spike_pairs
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_matches_reference_fixture(oracle, name):
+    net, t, c, nsteps, trace = build_case(name)
+    g = load_golden(name)
+    r = oracle.run(net, t, c, nsteps, trace=trace)
+    np.testing.assert_array_equal(spike_pairs(r["spike_step"], r["spike_cell"]),
+                                  spike_pairs(g["spike_step"], g["spike_cell"]))
+    nd = g["trace"].shape[2]
+    np.testing.assert_array_equal(r["trace"][:, :, :nd].astype(np.float32), g["trace"])
+    if "w_final" in g:
+        np.testing.assert_array_equal(r["w_final"].astype(np.float32), g["w_final"])
+    assert perm_digest(r["sorted_perm"]) == str(g["perm_sha256"])
+    assert r["n_events"] == int(g["counts"][1])
+    assert len(r["spike_step"]) == int(g["counts"][0])
+
+
+def test_fp64_oracle_is_close_to_float_mirror(oracle):
+    """The FP64 restatement (exact exp) stays close to the float32 mirror over the
+    first 100 ms of the recurrent LIF workload; this is the error yardstick."""
+    net, t, c, nsteps, trace = build_case("c1_lif_euler")
+    a = oracle.run(net, t, c, 1000, trace=(1000, 100, 16))
+    b = oracle.run(net, t, c, 1000, fp64=True, trace=(1000, 100, 16))
+    rms = float(np.sqrt(np.mean((a["trace"][:, :, 0] - b["trace"][:, :, 0]) ** 2)))
+    assert rms < 1e-2, rms
+
+
+def test_delay_rounding_matches_reference_rule(oracle):
+    # RoundPropagationDelay: floor(d*1e4 + 5e-5)*1e-4, minimum 1e-4 (Network.cpp:1311-1317)
+    assert oracle.round_delay(0.001) == 10 * 0.0001
+    assert oracle.round_delay(0.00149) == 14 * 0.0001
+    assert oracle.round_delay(0.00005) == 0.0001
+    assert oracle.round_delay(0.0) == 0.0001
+    assert oracle.round_delay(0.005) == 50 * 0.0001
