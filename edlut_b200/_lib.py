@@ -62,6 +62,9 @@ SIGNATURES = [
     ("eb_get_profile", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), c_i64p, c_f64p]),
     ("eb_launch_count", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
+    ("eb_fold_arrivals", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                         ctypes.c_void_p, ctypes.c_void_p]),
     ("eb_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("eb_restore", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
 ]

@@ -160,6 +160,23 @@ int eb_get_profile(eb_ctx *ctx, int cap, int *n, int *kind, int *pop, int64_t *l
 /* Number of library kernels launched so far (nodes of a replayed graph counted per replay). */
 int eb_launch_count(eb_ctx *ctx, int64_t *launches);
 
+/* ------------------------------------------------------ delivery op ---- */
+/* Fold a batch of n synaptic arrivals into conductance arrays in the reference's
+ * delivery order, on the device (stream: cudaStream_t as a pointer; enqueued, not
+ * synchronized).  All array arguments are device pointers.  Arrival i adds weight[i]
+ * to g_exc / g_inh / g_nmda (type[i] 0 / 1 / 2) of neuron target[i] < n_targets;
+ * per target the additions happen in order of (time[i], i) (time may be NULL: batch
+ * order), so the float sums round like the reference CPU models, which add each
+ * arrival straight into the conductance (NeuronModel::ProcessInputSpike,
+ * src/neuron_model/LIFTimeDrivenModel.cpp:77-83, event order
+ * src/spike/PropagatedSpikeGroup.cpp:112-149).  Replaces the per-arrival host
+ * accumulation of the GPU models (src/neuron_model/LIFTimeDrivenModel_GPU_C_INTERFACE.cu:66-70).
+ * Scratch memory is allocated per call on the stream (cudaMallocAsync).
+ * n_targets <= 1048576. */
+int eb_fold_arrivals(void *stream, int64_t n, const int32_t *target, const int8_t *type,
+                     const float *weight, const double *time, int64_t n_targets,
+                     float *g_exc, float *g_inh, float *g_nmda);
+
 /* ---------------------------------------------------- checkpoint/resume --- */
 /* Copy the whole dynamic state (neurons, BDF history, arrival buckets, weights,
  * plasticity traces, step counter) into an internal snapshot slot / restore it. */
