@@ -65,6 +65,10 @@ SIGNATURES = [
     ("eb_fold_arrivals", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
                                          ctypes.c_void_p, ctypes.c_void_p]),
+    ("eb_fold_arrivals_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                                 ctypes.c_void_p]),
     ("eb_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("eb_restore", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
 ]

@@ -12,7 +12,9 @@
 // (time, position in the batch), and added in that order.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <mutex>
 
 #include "edlut_b200.h"
 #include "eb_runtime.h"
@@ -171,4 +173,71 @@ extern "C" int eb_fold_arrivals(void *stream, int64_t n, const int32_t *target, 
     rc = fold_enqueue(st, scratch, n, target, type, weight, time, n_targets, g_exc, g_inh, g_nmda);
     cudaFreeAsync(scratch, st);
     return rc;
+}
+
+// ------------------------------------------------------ allocation-free form --
+// Some callers cannot allocate device memory while they run: a closed-loop
+// (real-time) controller whose step deadline must not contain allocator calls,
+// or a host engine that claims all device memory for itself at start-up.  This
+// form of the op takes its scratch from a fixed array in the library's device
+// image instead.  Every GPU that loads the library holds that array (about
+// 7 MiB) until the process exits; it bounds one call to kNoAllocMaxArrivals
+// arrivals and kNoAllocMaxTargets targets.  All calls share the one array and
+// it keeps the previous call's contents: the counters that must start at zero
+// are cleared at the start of every call, and two calls whose work overlaps on
+// the GPU (different streams, or different host threads on the same device)
+// race on it.
+namespace {
+
+constexpr int64_t kNoAllocMaxArrivals = 1 << 18;
+constexpr int64_t kNoAllocMaxTargets = 1 << 18;
+constexpr size_t kNoAllocScratchBytes =
+    (((3 * (size_t)(kNoAllocMaxTargets + 1) + kScanBlock) * sizeof(uint32_t) + 255) & ~(size_t)255) +
+    (size_t)kNoAllocMaxArrivals * sizeof(FoldRec);
+
+static __device__ __align__(256) unsigned char g_fold_scratch[kNoAllocScratchBytes];
+
+// The array's device address on each device, looked up once per device (with
+// that device current); in host code g_fold_scratch only names a host-side
+// stand-in, never the device memory.
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void *g_scratch_ptr[kMaxDevices] = {};
+
+int scratch_for_current_device(void **out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) { set_error("cudaGetDevice: %s", cudaGetErrorString(e)); return EB_ERR_CUDA; }
+    if (dev < 0 || dev >= kMaxDevices) { set_error("device index %d above %d", dev, kMaxDevices - 1); return EB_ERR_ARG; }
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_fold_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("cudaGetSymbolAddress(scratch) on device %d: %s", dev, cudaGetErrorString(e));
+            return EB_ERR_CUDA;
+        }
+        g_scratch_ptr[dev] = p;
+    }
+    *out = g_scratch_ptr[dev];
+    return EB_OK;
+}
+
+}  // namespace
+
+extern "C" int eb_fold_arrivals_noalloc(void *stream, int64_t n, const int32_t *target, const int8_t *type,
+                                        const float *weight, const double *time, int64_t n_targets,
+                                        float *g_exc, float *g_inh, float *g_nmda) {
+    int rc = fold_check(n, target, type, weight, n_targets);
+    if (rc) return rc;
+    if (n > kNoAllocMaxArrivals || n_targets > kNoAllocMaxTargets) {
+        set_error("eb_fold_arrivals_noalloc: %lld arrivals / %lld targets exceed its fixed scratch "
+                  "(at most %lld arrivals and %lld targets per call); use eb_fold_arrivals",
+                  (long long)n, (long long)n_targets, (long long)kNoAllocMaxArrivals, (long long)kNoAllocMaxTargets);
+        return EB_ERR_ARG;
+    }
+    void *scratch = nullptr;
+    if ((rc = scratch_for_current_device(&scratch))) return rc;
+    return fold_enqueue((cudaStream_t)stream, scratch, n, target, type, weight, time, n_targets, g_exc, g_inh,
+                        g_nmda);
 }

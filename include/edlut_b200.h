@@ -176,6 +176,19 @@ int eb_launch_count(eb_ctx *ctx, int64_t *launches);
 int eb_fold_arrivals(void *stream, int64_t n, const int32_t *target, const int8_t *type,
                      const float *weight, const double *time, int64_t n_targets,
                      float *g_exc, float *g_inh, float *g_nmda);
+/* The same fold without any allocation, for callers that cannot allocate device
+ * memory while they run (a closed-loop real-time controller whose step deadline
+ * must not contain allocator calls, or a host engine that claims all device memory
+ * at start-up).  No counterpart in the reference.  Its scratch is a fixed array in
+ * the library's device image (about 7 MiB, held on every GPU that loads the library
+ * until exit), so one call takes at most 262144 arrivals and 262144 targets; larger
+ * batches return EB_ERR_ARG.  It runs on the calling thread's current device; the
+ * first call on a device looks up that array's address (cudaGetSymbolAddress) and
+ * should come before any stream capture.  All calls share the array: calls whose
+ * GPU work overlaps (other streams or threads on the same device) race. */
+int eb_fold_arrivals_noalloc(void *stream, int64_t n, const int32_t *target, const int8_t *type,
+                             const float *weight, const double *time, int64_t n_targets,
+                             float *g_exc, float *g_inh, float *g_nmda);
 
 /* ---------------------------------------------------- checkpoint/resume --- */
 /* Copy the whole dynamic state (neurons, BDF history, arrival buckets, weights,
