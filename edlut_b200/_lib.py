@@ -45,6 +45,9 @@ SIGNATURES = [
     ("eb_run_async", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
     ("eb_sync", ctypes.c_int, [ctypes.c_void_p]),
     ("eb_set_graph_steps", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("eb_set_persistent", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("eb_set_timeline", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("eb_get_timeline", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_void_p]),
     ("eb_set_record_capacity", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
     ("eb_get_spikes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_i64p, c_i64p, c_i64p]),
     ("eb_step_time", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_f64p]),

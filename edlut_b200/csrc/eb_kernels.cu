@@ -160,13 +160,12 @@ __device__ __forceinline__ void compact_spikes(const PopDev &P, const NetDev &N,
 // One thread per neuron.  Arrivals of this step are sorted in registers
 // (insertion sort; at most 16 in the fast path) and folded in order.
 constexpr int kLocalSort = 16;
+constexpr int kNarrowTile = 256;
 
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(256) k_update_narrow(PopDev P, NetDev N, int rel) {
+__device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev &N, int64_t k, int64_t tile) {
     constexpr int ND = Model<KIND>::ND;
-    const int64_t k = cur_step(N, rel);
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
+    const int64_t i = tile * kNarrowTile + threadIdx.x;
     const bool active = i < P.n;
     bool sp = false;
     uint32_t c = 0;
@@ -215,6 +214,13 @@ __global__ void __launch_bounds__(256) k_update_narrow(PopDev P, NetDev N, int r
     compact_spikes(P, N, k, i, sp);
 }
 
+template <int KIND, int INTEG>
+__global__ void __launch_bounds__(kNarrowTile) k_update_narrow(PopDev P, NetDev N, int rel) {
+    const int64_t k = cur_step(N, rel);
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
+    update_narrow_tile<KIND, INTEG>(P, N, k, blockIdx.x);
+}
+
 // ------------------------------------------------------------- wide update --
 // One block per neuron, for populations whose neurons receive many arrivals per
 // step (e.g. Purkinje-like cells with 10^4-10^5 inputs).  The block sorts the
@@ -226,99 +232,189 @@ __global__ void __launch_bounds__(256) k_update_narrow(PopDev P, NetDev N, int r
 constexpr int kWideThreads = 256;
 constexpr int kWideSmem = 1024;
 
+constexpr int kRankSort = 256;  // up to this many arrivals: rank sort (one pass), else bitonic
+
+struct WideSmem {
+    Arrival sbuf[kWideSmem];
+    Arrival sorted[kRankSort];
+    float sw[kWideSmem];
+    uint8_t sty[kWideSmem];
+};
+
+// STDP pre hook for one arrival with every synapse load issued up front (they
+// only depend on tp); returns the weight before the update through w_old.
+__device__ __forceinline__ void stdp_pre_gather(const NetDev &N, uint32_t tp, double a, float &w_old, int &ty) {
+    const float w = N.w[tp];
+    const int t8 = N.stype[tp];
+    const int rl = N.rule[tp];
+    const double last = N.last[tp];
+    const float pre0 = N.pre[tp], post0 = N.post[tp], mw = N.maxw[tp];
+    w_old = w;
+    ty = t8;
+    if (rl < 0) return;
+    const float *rp = N.rule_par + rl * 6;
+    const float el = (float)(a - last);
+    float pre = pre0 * expt_net(N, -el * rp[4]);
+    float post = post0 * expt_net(N, -el * rp[5]);
+    pre += 1.0f;
+    float wn = w;
+    wn += -rp[2] * post;
+    if (wn > mw) wn = mw; else if (wn < 0.0f) wn = 0.0f;
+    N.last[tp] = a;
+    N.pre[tp] = pre;
+    N.post[tp] = post;
+    N.w[tp] = wn;
+}
+
+// Add c weights to the conductances in order.  Each conductance only sees its
+// own type's weights, in order, so selecting per element reproduces the
+// interleaved sequential sum; loads are batched ahead of the dependent adds.
+template <int ND>
+__device__ __forceinline__ void ordered_sum(float *x, const float *sw, const uint8_t *sty, uint32_t c) {
+    float ge = x[ND], gi = x[ND + 1], gn = x[ND + 2];
+    uint32_t a = 0;
+    for (; a + 8 <= c; a += 8) {
+        float w[8];
+        int t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) { w[u] = sw[a + u]; t[u] = sty[a + u]; }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            ge = (t[u] == 0) ? ge + w[u] : ge;
+            gi = (t[u] == 1) ? gi + w[u] : gi;
+            gn = (t[u] == 2) ? gn + w[u] : gn;
+        }
+    }
+    for (; a < c; ++a) {
+        const float w = sw[a];
+        const int t = sty[a];
+        ge = (t == 0) ? ge + w : ge;
+        gi = (t == 1) ? gi + w : gi;
+        gn = (t == 2) ? gn + w : gn;
+    }
+    x[ND] = ge;
+    x[ND + 1] = gi;
+    x[ND + 2] = gn;
+}
+
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel) {
+__device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S) {
     constexpr int ND = Model<KIND>::ND;
-    __shared__ Arrival sbuf[kWideSmem];
-    __shared__ float sw[kWideSmem];
-    __shared__ uint8_t sty[kWideSmem];
     const int tid = threadIdx.x;
-    const int64_t k = cur_step(N, rel);
-    if (blockIdx.x == 0 && tid == 0) P.spk_count[(k + 1) & 1] = 0;
     const int slot = (int)(k % N.R);
-    for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) {
-        const int64_t gi = P.first + i;
-        uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
-        uint32_t c = *cp;
-        __syncthreads();
-        float x[kMaxVars];
-        if (tid == 0) load_state<KIND>(P, i, x);
-        if (c) {
-            if (tid == 0) *cp = 0;
-            const uint32_t capg = N.cap[gi];
-            if (c > capg) { if (tid == 0) atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
-            Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
-            if (c <= (uint32_t)kWideSmem) {
+    const int64_t gi = P.first + i;
+    uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
+    uint32_t c = *cp;
+    __syncthreads();
+    float x[kMaxVars];
+    if (tid == 0) load_state<KIND>(P, i, x);
+    if (c) {
+        if (tid == 0) *cp = 0;
+        const uint32_t capg = N.cap[gi];
+        if (c > capg) { if (tid == 0) atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
+        Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
+        if (c <= (uint32_t)kWideSmem) {
+            const Arrival *ord;
+            if (c <= (uint32_t)kRankSort) {
+                // rank sort: position of each arrival = number of arrivals before it in
+                // (time, synapse order, bucket index) order; one pass, all keys distinct
+                for (int a = tid; a < (int)c; a += blockDim.x) S.sbuf[a] = r[a];
+                __syncthreads();
+                for (int a = tid; a < (int)c; a += blockDim.x) {
+                    const Arrival v = S.sbuf[a];
+                    int rank = 0;
+                    for (int b = 0; b < (int)c; ++b) {
+                        const Arrival u = S.sbuf[b];
+                        rank += (arr_less(u, v) || (!arr_less(v, u) && b < a)) ? 1 : 0;
+                    }
+                    S.sorted[rank] = v;
+                }
+                __syncthreads();
+                ord = S.sorted;
+            } else {
                 int n2 = 1;
                 while (n2 < (int)c) n2 <<= 1;
-                for (int a = tid; a < n2; a += kWideThreads) {
-                    if (a < (int)c) sbuf[a] = r[a];
-                    else { sbuf[a].a = __longlong_as_double(0x7ff0000000000000LL); sbuf[a].spos = 0xffffffffu; sbuf[a].tpos = 0; }
+                for (int a = tid; a < n2; a += blockDim.x) {
+                    if (a < (int)c) S.sbuf[a] = r[a];
+                    else { S.sbuf[a].a = __longlong_as_double(0x7ff0000000000000LL); S.sbuf[a].spos = 0xffffffffu; S.sbuf[a].tpos = 0; }
                 }
                 __syncthreads();
                 for (int size = 2; size <= n2; size <<= 1)
                     for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                        for (int a = tid; a < n2; a += kWideThreads) {
+                        for (int a = tid; a < n2; a += blockDim.x) {
                             const int b = a ^ stride;
                             if (b > a) {
                                 const bool up = ((a & size) == 0);
-                                const Arrival ea = sbuf[a], eb = sbuf[b];
-                                if (up ? arr_less(eb, ea) : arr_less(ea, eb)) { sbuf[a] = eb; sbuf[b] = ea; }
+                                const Arrival ea = S.sbuf[a], eb = S.sbuf[b];
+                                if (up ? arr_less(eb, ea) : arr_less(ea, eb)) { S.sbuf[a] = eb; S.sbuf[b] = ea; }
                             }
                         }
                         __syncthreads();
                     }
-                if (P.may_repeat) {
-                    if (tid == 0)
-                        for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, sbuf[a], x);
-                } else {
-                    for (int a = tid; a < (int)c; a += kWideThreads) {
-                        const Arrival v = sbuf[a];
-                        const uint32_t tp = v.tpos;
-                        sw[a] = N.w[tp];
-                        sty[a] = N.stype[tp];
-                        const int rl = N.rule[tp];
-                        if (rl >= 0) stdp_pre(N, tp, rl, v.a);
-                    }
-                    __syncthreads();
-                    if (tid == 0)
-                        for (uint32_t a = 0; a < c; ++a) add_conductance<ND>(x, sty[a], sw[a]);
-                }
-            } else if (tid == 0) {
-                for (uint32_t a = 1; a < c; ++a) {  // rare: insertion sort in global memory
-                    Arrival v = r[a];
-                    int b = (int)a - 1;
-                    while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
-                    r[b + 1] = v;
-                }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, r[a], x);
+                ord = S.sbuf;
             }
-            if (tid == 0) atomicAdd(N.events, (unsigned long long)c);
-        }
-        if (tid == 0) {
-            const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x);
-            store_state<KIND>(P, i, x);
-            record_trace(P, N, k, gi, x, Model<KIND>::NV);
-            if (sp) {
-                const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
-                if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
-                else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
-                if (N.rec_buf) {
-                    const unsigned long long ro = atomicAdd(N.rec_count, 1ull);
-                    if (ro < (unsigned long long)N.rec_cap)
-                        N.rec_buf[ro] = ((unsigned long long)k << 32) | (unsigned long long)gi;
-                    else atomicOr(N.flags, FLAG_RECORD_OVERFLOW);
+            if (P.may_repeat) {
+                if (tid == 0)
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, ord[a], x);
+            } else {
+                for (int a = tid; a < (int)c; a += blockDim.x) {
+                    const Arrival v = ord[a];
+                    float w_old;
+                    int ty;
+                    stdp_pre_gather(N, v.tpos, v.a, w_old, ty);
+                    S.sw[a] = w_old;
+                    S.sty[a] = (uint8_t)ty;
                 }
+                __syncthreads();
+                if (tid == 0) ordered_sum<ND>(x, S.sw, S.sty, c);
+            }
+        } else if (tid == 0) {
+            for (uint32_t a = 1; a < c; ++a) {  // rare: insertion sort in global memory
+                Arrival v = r[a];
+                int b = (int)a - 1;
+                while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
+                r[b + 1] = v;
+            }
+            for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, r[a], x);
+        }
+        if (tid == 0) atomicAdd(N.events, (unsigned long long)c);
+    }
+    if (tid == 0) {
+        const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x);
+        store_state<KIND>(P, i, x);
+        record_trace(P, N, k, gi, x, Model<KIND>::NV);
+        if (sp) {
+            const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
+            if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
+            else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
+            if (N.rec_buf) {
+                const unsigned long long ro = atomicAdd(N.rec_count, 1ull);
+                if (ro < (unsigned long long)N.rec_cap)
+                    N.rec_buf[ro] = ((unsigned long long)k << 32) | (unsigned long long)gi;
+                else atomicOr(N.flags, FLAG_RECORD_OVERFLOW);
             }
         }
     }
+    __syncthreads();
+}
+
+template <int KIND, int INTEG>
+__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel) {
+    __shared__ WideSmem S;
+    const int64_t k = cur_step(N, rel);
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
+    for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) update_wide_neuron<KIND, INTEG>(P, N, k, i, S);
 }
 
 // ------------------------------------------------------------ spike fan-out --
-// Arrival step of a delivery at time a: the first update time strictly after a.
-// `est` is a close guess; two table reads confirm it in the common case.
-__device__ __forceinline__ int64_t arrival_step(const NetDev &N, double a, int64_t k_lo, int64_t est) {
-    int64_t ka = est < k_lo ? k_lo : est;
+// Arrival step of a delivery at time a: the first update time strictly after a
+// (never below k_lo).  The guess floor(a/dt)+1 is confirmed by two independent
+// table reads in the common case; the loops only run when it is off by rounding.
+__device__ __forceinline__ int64_t arrival_step(const NetDev &N, double a, int64_t k_lo, double inv_dt) {
+    int64_t ka = (int64_t)(a * inv_dt) + 1;
+    if (ka < k_lo) ka = k_lo;
+    const double lo = N.tstep[ka - 1], hi = N.tstep[ka];
+    if (hi > a && (lo <= a || ka == k_lo)) return ka;
     while (N.tstep[ka] <= a) ++ka;
     while (ka > k_lo && N.tstep[ka - 1] > a) --ka;
     return ka;
@@ -344,74 +440,330 @@ __device__ __forceinline__ void bucket_put(const NetDev &N, int64_t ka, double a
     }
 }
 
-// Spikes of population P at step k (update time t_k): one block per spike, the
-// threads cover the source's out-synapses (sorted by delay, then target).
+// One spike of population P at step k (update time t_k): the block's threads
+// cover the source's out-synapses (sorted by delay, then target).
+__device__ __forceinline__ void push_spike(const PopDev &P, const NetDev &N, int64_t k, int64_t s, double inv_dt) {
+    const double tk = N.tstep[k];
+    const int64_t src = P.first + P.spk[s];
+    const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
+    for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
+        const double a = tk + (double)N.out_units[o] * 0.0001;
+        bucket_put(N, arrival_step(N, a, k + 1, inv_dt), a, o);
+    }
+}
+
+// One input-neuron spike q emitted in [t_{k-1}, t_k).  A source with several
+// distinct delays delivers group j+1 at (a_j - d_j) + d_{j+1}, as the reference's
+// PropagatedSpike chain does.
+__device__ __forceinline__ void input_spike(const NetDev &N, int64_t k, int64_t q, double inv_dt) {
+    const int64_t src = N.in_cell[q];
+    const double tin = N.in_time[q];
+    const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
+    const int64_t g0 = N.grp_ptr[src], g1 = N.grp_ptr[src + 1];
+    for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
+        const uint16_t u = N.out_units[o];
+        double a = tin + (double)N.grp_units[g0] * 0.0001;
+        for (int64_t g = g0 + 1; g < g1 && N.grp_units[g - 1] != u; ++g)
+            a = a - (double)N.grp_units[g - 1] * 0.0001 + (double)N.grp_units[g] * 0.0001;
+        bucket_put(N, arrival_step(N, a, k, inv_dt), a, o);
+    }
+}
+
+// Post-synaptic STDP (STDPWeightChange::ApplyPostSynapticSpike) for work item
+// (spike s, chunk ch of blockDim plastic inputs): one synapse per thread.
+__device__ __forceinline__ void post_item(const PopDev &P, const NetDev &N, int64_t k, int64_t s, int64_t ch) {
+    const double tk = N.tstep[k];
+    const int64_t t = P.first + P.spk[s];
+    const int64_t tp = N.in_ptr[t] + ch * blockDim.x + threadIdx.x;
+    if (tp >= N.plastic_end[t]) return;
+    const int rl = N.rule[tp];
+    const float *rp = N.rule_par + rl * 6;
+    const double last = N.last[tp];
+    float pre = N.pre[tp], post = N.post[tp], w = N.w[tp];
+    const float mw = N.maxw[tp];
+    const float el = (float)(tk - last);
+    pre *= expt_net(N, -el * rp[4]);
+    post *= expt_net(N, -el * rp[5]);
+    post += 1.0f;
+    w += rp[0] * pre;
+    if (w > mw) w = mw; else if (w < 0.0f) w = 0.0f;
+    N.last[tp] = tk;
+    N.pre[tp] = pre;
+    N.post[tp] = post;
+    N.w[tp] = w;
+}
+
 __global__ void __launch_bounds__(256) k_push(PopDev P, NetDev N, int rel, double inv_dt) {
     const int64_t k = cur_step(N, rel);
     const uint32_t ns = min(P.spk_count[k & 1], (uint32_t)P.n);
-    const double tk = N.tstep[k];
-    for (int64_t s = blockIdx.x; s < ns; s += gridDim.x) {
-        const int64_t src = P.first + P.spk[s];
-        const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
-        for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-            const double d = (double)N.out_units[o] * 0.0001;
-            const double a = tk + d;
-            bucket_put(N, arrival_step(N, a, k + 1, k + (int64_t)(d * inv_dt)), a, o);
-        }
-    }
+    for (int64_t s = blockIdx.x; s < ns; s += gridDim.x) push_spike(P, N, k, s, inv_dt);
 }
 
-// Input-neuron spikes emitted in [t_{k-1}, t_k): one block per spike.  A source
-// with several distinct delays delivers group j+1 at (a_j - d_j) + d_{j+1}, as the
-// reference's PropagatedSpike chain does.
 __global__ void __launch_bounds__(256) k_input_push(NetDev N, int rel, double inv_dt) {
     const int64_t k = cur_step(N, rel);
     const int64_t q0 = N.in_start[k], q1 = N.in_start[k + 1];
-    const double tprev = N.tstep[k - 1];
-    for (int64_t q = q0 + blockIdx.x; q < q1; q += gridDim.x) {
-        const int64_t src = N.in_cell[q];
-        const double tin = N.in_time[q];
-        const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
-        const int64_t g0 = N.grp_ptr[src], g1 = N.grp_ptr[src + 1];
-        for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-            const uint16_t u = N.out_units[o];
-            double a = tin + (double)N.grp_units[g0] * 0.0001;
-            for (int64_t g = g0 + 1; g < g1 && N.grp_units[g - 1] != u; ++g)
-                a = a - (double)N.grp_units[g - 1] * 0.0001 + (double)N.grp_units[g] * 0.0001;
-            bucket_put(N, arrival_step(N, a, k, k - 1 + (int64_t)((a - tprev) * inv_dt)), a, o);
-        }
-    }
+    for (int64_t q = q0 + blockIdx.x; q < q1; q += gridDim.x) input_spike(N, k, q, inv_dt);
 }
 
-// Post-synaptic STDP (STDPWeightChange::ApplyPostSynapticSpike) for every spike
-// of population P at step k.  Work items are (spike, chunk of blockDim plastic
-// input synapses of that neuron); one synapse per thread.
 __global__ void __launch_bounds__(256) k_post_stdp(PopDev P, NetDev N, int rel, int max_chunks) {
     const int64_t k = cur_step(N, rel);
     const uint32_t ns = min(P.spk_count[k & 1], (uint32_t)P.n);
-    const double tk = N.tstep[k];
     const int64_t items = (int64_t)ns * max_chunks;
-    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const int64_t s = item / max_chunks, ch = item % max_chunks;
-        const int64_t t = P.first + P.spk[s];
-        const int64_t tp = N.in_ptr[t] + ch * blockDim.x + threadIdx.x;
-        if (tp >= N.plastic_end[t]) continue;
-        const int rl = N.rule[tp];
-        const float *rp = N.rule_par + rl * 6;
-        const double last = N.last[tp];
-        float pre = N.pre[tp], post = N.post[tp], w = N.w[tp];
-        const float mw = N.maxw[tp];
-        const float el = (float)(tk - last);
-        pre *= expt_net(N, -el * rp[4]);
-        post *= expt_net(N, -el * rp[5]);
-        post += 1.0f;
-        w += rp[0] * pre;
-        if (w > mw) w = mw; else if (w < 0.0f) w = 0.0f;
-        N.last[tp] = tk;
-        N.pre[tp] = pre;
-        N.post[tp] = post;
-        N.w[tp] = w;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) post_item(P, N, k, item / max_chunks, item % max_chunks);
+}
+
+// -------------------------------------------------------- persistent kernel --
+// All phases of K consecutive steps in one cooperative launch.  Per step:
+//   [inputs]  input-spike fan-out (its own phase only when an input delivery can
+//             reach the step being updated)
+//   phase A   neuron updates of every population (+ input fan-out when it cannot
+//             reach this step): narrow tiles of 256 neurons / one block per
+//             wide neuron, items spread over the blocks
+//   phase B   post-synaptic STDP chunks and spike fan-out of every population
+// separated by grid barriers.  Removes the per-launch cost (about 3 us per
+// kernel on this part) and the graph dependency latency of the K x (2..3)
+// launches it replaces.  Every barrier wait is bounded: on timeout the block
+// records FLAG_BARRIER_TIMEOUT and the kernel ends.
+constexpr unsigned long long kBarrierSpinLimit = 1ull << 24;
+constexpr int kTlSlots = 6;
+constexpr int kBarrierGroup = 16;     // blocks per first-level counter
+constexpr int kBarrierStride = 32;    // words between counters (own 128-byte line)
+
+// Two-level grid barrier: blocks arrive on the counter of their group of
+// kBarrierGroup; the last of a group arrives on the root counter; the last at
+// the root resets the counters and advances the generation word every block
+// polls.  Spreads the arrival atomics over many cache lines instead of
+// serialising gridDim.x of them on one.  Layout of bar (words):
+//   [0] generation, [kBarrierStride] root count, [(g+2)*kBarrierStride] group g.
+__device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned nblocks, uint32_t *flags) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        volatile unsigned *gen = bar;
+        const unsigned g = *gen;
+        const unsigned grp = blockIdx.x / kBarrierGroup;
+        const unsigned ngroups = (nblocks + kBarrierGroup - 1) / kBarrierGroup;
+        const unsigned in_grp = min((unsigned)kBarrierGroup, nblocks - grp * kBarrierGroup);
+        unsigned *gc = bar + (grp + 2) * kBarrierStride;
+        unsigned *root = bar + kBarrierStride;
+        __threadfence();
+        bool last = false;
+        if (atomicAdd(gc, 1u) == in_grp - 1) {
+            *gc = 0;
+            __threadfence();
+            if (atomicAdd(root, 1u) == ngroups - 1) {
+                *root = 0;
+                last = true;
+            }
+        }
+        if (last) {
+            __threadfence();
+            atomicAdd(bar, 1u);
+        } else {
+            unsigned long long spins = 0;
+            while (*gen == g) {
+                __nanosleep(32);
+                if (++spins > kBarrierSpinLimit) {
+                    atomicOr(flags, FLAG_BARRIER_TIMEOUT);
+                    s_ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence();
     }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+template <int KIND, int INTEG>
+__device__ __forceinline__ void update_item(const PopDev &P, const NetDev &N, int64_t k, int64_t local, WideSmem &S) {
+    if (P.wide) update_wide_neuron<KIND, INTEG>(P, N, k, local, S);
+    else update_narrow_tile<KIND, INTEG>(P, N, k, local);
+}
+
+// Register classes of the persistent kernel: the switch below compiles in only
+// the model/integrator pairs of its class, so a network without HH or BDF does
+// not pay their register pressure.
+//   0: LIF, AdEx x Euler, RK2, RK4   1: + HH x Euler, RK2, RK4   2: everything
+template <int CLASS, int KIND>
+__device__ __forceinline__ void update_item_k(const PopDev &P, const NetDev &N, int64_t k, int64_t local, WideSmem &S) {
+    switch (P.integ) {
+    case INTEG_EULER: update_item<KIND, INTEG_EULER>(P, N, k, local, S); break;
+    case INTEG_RK2: update_item<KIND, INTEG_RK2>(P, N, k, local, S); break;
+    case INTEG_RK4: update_item<KIND, INTEG_RK4>(P, N, k, local, S); break;
+    default:
+        if constexpr (CLASS >= 2) update_item<KIND, INTEG_BDF>(P, N, k, local, S);
+        else if (threadIdx.x == 0) atomicOr(N.flags, FLAG_BARRIER_TIMEOUT);
+        break;
+    }
+}
+
+int persist_class_of(int kind, int integ) {
+    if (integ == INTEG_BDF) return 2;
+    return kind == KIND_HH ? 1 : 0;
+}
+
+__device__ __forceinline__ int64_t update_items(const PopDev &P) {
+    return P.wide ? P.n : (P.n + kNarrowTile - 1) / kNarrowTile;
+}
+
+// The item code reads its population's parameters many times per neuron; a
+// block keeps the descriptor of the population it is working on in shared
+// memory (broadcast reads) and reloads it only when it moves to another one.
+__device__ __forceinline__ const PopDev &stage_pop(const PopDev *pops, int q, PopDev &sp, int &cur) {
+    if (cur != q) {
+        __syncthreads();
+        const int *src = reinterpret_cast<const int *>(pops + q);
+        int *dst = reinterpret_cast<int *>(&sp);
+        for (int w = threadIdx.x; w < (int)(sizeof(PopDev) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+        __syncthreads();
+        cur = q;
+    }
+    return sp;
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Optional timeline (I.tl): per step r < I.tl_steps and block b, globaltimer at
+// phase start, phase-A barrier arrival, phase-A barrier exit, phase-B barrier arrival.
+__device__ __forceinline__ void tl_mark(const PersistInfo &I, int r, int slot) {
+    if (I.tl && r < I.tl_steps && threadIdx.x == 0) I.tl[((int64_t)r * kTlSlots + slot) * gridDim.x + blockIdx.x] = gtimer();
+}
+__device__ __forceinline__ void tl_put(const PersistInfo &I, int r, int slot, unsigned long long v) {
+    if (I.tl && r < I.tl_steps && threadIdx.x == 0) I.tl[((int64_t)r * kTlSlots + slot) * gridDim.x + blockIdx.x] = v;
+}
+
+// Dynamic item queue of one phase: each block starts with item blockIdx.x and
+// then takes the next free index from the phase's counter (gridDim.x + n), so a
+// block held up by a long item (a wide neuron) does not also receive later items.
+// Thread 0 requests the following index as soon as it starts an item, hiding the
+// atomic's latency behind the item's work.
+struct ItemQueue {
+    unsigned long long *ctr;
+    int64_t cur, next;
+    __device__ __forceinline__ void begin(unsigned long long *c) {
+        ctr = c;
+        cur = blockIdx.x;
+    }
+    __device__ __forceinline__ void prefetch() {
+        if (threadIdx.x == 0) next = (int64_t)gridDim.x + (int64_t)atomicAdd(ctr, 1ull);
+    }
+    __device__ __forceinline__ int64_t advance(int64_t *s_next) {
+        __syncthreads();
+        if (threadIdx.x == 0) *s_next = next;
+        __syncthreads();
+        cur = *s_next;
+        return cur;
+    }
+};
+
+template <int CLASS>
+__global__ void __launch_bounds__(kNarrowTile, CLASS == 0 ? 3 : (CLASS == 1 ? 2 : 1)) k_persistent(const PopDev *__restrict__ pops, PersistInfo I, NetDev N,
+                                                            int K) {
+    __shared__ WideSmem S;
+    __shared__ PopDev sp;
+    __shared__ int64_t s_next;
+    int cur = -1;
+    ItemQueue Q;
+    const int64_t base = *N.step;
+    const unsigned nb = gridDim.x;
+    for (int r = 0; r < K; ++r) {
+        const int64_t k = base + r + 1;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            for (int q = 0; q < I.n_pops; ++q) pops[q].spk_count[(k + 1) & 1] = 0;
+            I.queue[(((k + 1) & 1) * 2 + 0) * 16] = 0;  // counters of the next step's phases
+            I.queue[(((k + 1) & 1) * 2 + 1) * 16] = 0;
+        }
+        int64_t n_in = 0, q0 = 0;
+        if (I.has_inputs) { q0 = N.in_start[k]; n_in = N.in_start[k + 1] - q0; }
+        if (I.has_inputs && !I.inputs_concurrent) {
+            for (int64_t it = blockIdx.x; it < n_in; it += nb) input_spike(N, k, q0 + it, I.inv_dt);
+            if (!grid_sync(I.bar, nb, N.flags)) return;
+            n_in = 0;
+        }
+        // phase A: longest items first -- the populations in I.order (wide ones
+        // first), with the input fan-out after the wide populations
+        tl_mark(I, r, 0);
+        int64_t total = n_in;
+        for (int q = 0; q < I.n_pops; ++q) total += update_items(pops[q]);
+        int n_items = 0;
+        Q.begin(I.queue + ((k & 1) * 2 + 0) * 16);
+        for (int64_t it = Q.cur; it < total; it = Q.advance(&s_next)) {
+            Q.prefetch();
+            if (n_items == 1) tl_mark(I, r, 4);
+            ++n_items;
+            int64_t local = it;
+            int j = 0, q = -1;
+            for (; j < I.n_pops; ++j) {
+                if (j == I.n_wide) {
+                    if (local < n_in) break;
+                    local -= n_in;
+                }
+                const int64_t ni = update_items(pops[I.order[j]]);
+                if (local < ni) { q = I.order[j]; break; }
+                local -= ni;
+            }
+            if (q < 0) { input_spike(N, k, q0 + local, I.inv_dt); continue; }  // (advance runs in the for header)
+            const PopDev &P = stage_pop(pops, q, sp, cur);
+            switch (P.kind) {
+            case KIND_LIF: update_item_k<CLASS, KIND_LIF>(P, N, k, local, S); break;
+            case KIND_ADEX: update_item_k<CLASS, KIND_ADEX>(P, N, k, local, S); break;
+            default:
+                if constexpr (CLASS >= 1) update_item_k<CLASS, KIND_HH>(P, N, k, local, S);
+                break;
+            }
+        }
+        tl_mark(I, r, 1);
+        tl_put(I, r, 5, (unsigned long long)n_items);
+        if (!grid_sync(I.bar, nb, N.flags)) return;
+        tl_mark(I, r, 2);
+        // phase B
+        int64_t cnt[kMaxPersistPops];
+        total = 0;
+        for (int q = 0; q < I.n_pops; ++q) {
+            const int64_t ns = min((int64_t)pops[q].spk_count[k & 1], pops[q].n);
+            cnt[q] = ns * ((I.has_plastic >> q) & 1 ? I.post_chunks[q] : 0) + ns * ((I.has_out >> q) & 1);
+            total += cnt[q];
+        }
+        Q.begin(I.queue + ((k & 1) * 2 + 1) * 16);
+        for (int64_t it = Q.cur; it < total; it = Q.advance(&s_next)) {
+            Q.prefetch();
+            int64_t local = it;
+            int q = 0;
+            while (local >= cnt[q]) { local -= cnt[q]; ++q; }
+            const PopDev &P = stage_pop(pops, q, sp, cur);
+            const int64_t np = ((I.has_plastic >> q) & 1) ? min((int64_t)P.spk_count[k & 1], P.n) * I.post_chunks[q] : 0;
+            if (local < np) post_item(P, N, k, local / I.post_chunks[q], local % I.post_chunks[q]);
+            else push_spike(P, N, k, local - np, I.inv_dt);
+        }
+        tl_mark(I, r, 3);
+        if (!grid_sync(I.bar, nb, N.flags)) return;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *const_cast<int64_t *>(N.step) += K;
+}
+
+static const void *persist_fn(int cls) {
+    if (cls == 0) return (const void *)k_persistent<0>;
+    if (cls == 1) return (const void *)k_persistent<1>;
+    return (const void *)k_persistent<2>;
+}
+
+int persistent_blocks_per_sm(int cls) {
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, persist_fn(cls), kNarrowTile, 0);
+    return nb;
+}
+
+cudaError_t launch_persistent(int cls, const PopDev *pops, const PersistInfo &I, const NetDev &N, int K, int grid,
+                              cudaStream_t st) {
+    void *args[] = {(void *)&pops, (void *)&I, (void *)&N, (void *)&K};
+    return cudaLaunchCooperativeKernel(persist_fn(cls), dim3(grid), dim3(kNarrowTile), args, 0, st);
 }
 
 __global__ void k_advance(int64_t *step, int K) { *step += K; }

@@ -10,4 +10,24 @@ void launch_push(const PopDev &P, const NetDev &N, int rel, double inv_dt, int b
 void launch_input_push(const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st);
 void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks, int blocks, cudaStream_t st);
 void launch_advance(int64_t *step, int K, cudaStream_t st);
+
+constexpr int kMaxPersistPops = 16;
+// Host-built description of one network for the persistent kernel.
+struct PersistInfo {
+    int n_pops;                       // model populations (PopDev array order)
+    int has_inputs, inputs_concurrent;
+    unsigned has_out, has_plastic;    // bit q: population q
+    int post_chunks[kMaxPersistPops];
+    double inv_dt;
+    int order[kMaxPersistPops];       // phase-A population order (wide populations first)
+    int n_wide;                       // number of wide populations at the front of order
+    unsigned *bar;                    // grid barrier words (generation, root, group counters)
+    unsigned long long *queue;        // item counters [step parity][phase], 128 bytes apart
+    unsigned long long *tl;           // optional timeline [tl_steps][4][grid] (globaltimer ns)
+    int tl_steps;
+};
+int persist_class_of(int kind, int integ);
+int persistent_blocks_per_sm(int cls);
+cudaError_t launch_persistent(int cls, const PopDev *pops, const PersistInfo &I, const NetDev &N, int K, int grid,
+                              cudaStream_t st);
 }  // namespace eb

@@ -416,6 +416,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         fork_ev.push_back(a);
         join_ev.push_back(b);
     }
+    if ((rc = setup_persistent())) return rc;
     CK(cudaStreamSynchronize(st));
     finalized = true;
     steps_done = 0;
@@ -615,6 +616,58 @@ void eb_ctx::enqueue_step(int rel) {
     fork_join(phase);
 }
 
+// Decide whether the persistent kernel can run this network and prepare its
+// arguments: at most kMaxPersistPops model populations, cooperative launch
+// support, and at least one resident block per SM.
+int eb_ctx::setup_persistent() {
+    persist_ok = false;
+    int coop = 0, nsm = 0;
+    CK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    int n_model = 0;
+    persist_class = 0;
+    memset(&pinfo, 0, sizeof(pinfo));
+    for (auto &p : pops) {
+        if (p.kind == KIND_INPUT) continue;
+        if (n_model < kMaxPersistPops) {
+            if (p.has_out) pinfo.has_out |= 1u << n_model;
+            if (p.has_plastic_in) pinfo.has_plastic |= 1u << n_model;
+            pinfo.post_chunks[n_model] = std::max(1, p.post_chunks);
+        }
+        persist_class = std::max(persist_class, persist_class_of(p.kind, p.integ));
+        n_model++;
+    }
+    if (!coop || n_model == 0 || n_model > kMaxPersistPops) return EB_OK;
+    const int bps = persistent_blocks_per_sm(persist_class);
+    if (bps < 1) return EB_OK;
+    persist_grid = bps * nsm;
+    pinfo.n_pops = n_model;
+    {
+        int j = 0, q = 0;
+        std::vector<int> wide, narrow;
+        for (auto &p : pops) {
+            if (p.kind == KIND_INPUT) continue;
+            (p.dev.wide ? wide : narrow).push_back(q++);
+        }
+        for (int w : wide) pinfo.order[j++] = w;
+        for (int w : narrow) pinfo.order[j++] = w;
+        pinfo.n_wide = (int)wide.size();
+    }
+    pinfo.has_inputs = has_inputs ? 1 : 0;
+    pinfo.inputs_concurrent = inputs_concurrent ? 1 : 0;
+    pinfo.inv_dt = 1.0 / dt_s;
+    int rc;
+    const size_t bar_words = (size_t)((persist_grid + 15) / 16 + 2) * 32;  // generation, root, one line per group
+    if ((rc = dalloc((void **)&pinfo.bar, bar_words * sizeof(unsigned)))) return rc;
+    CK(cudaMemsetAsync(pinfo.bar, 0, bar_words * sizeof(unsigned), stream));
+    if ((rc = dalloc((void **)&d_pops, sizeof(PopDev) * (size_t)n_model))) return rc;
+    if ((rc = dalloc((void **)&pinfo.queue, 4 * 16 * sizeof(unsigned long long)))) return rc;
+    CK(cudaMemsetAsync(pinfo.queue, 0, 4 * 16 * sizeof(unsigned long long), stream));
+    pops_dirty = true;
+    persist_ok = true;
+    return EB_OK;
+}
+
 int eb_ctx::build_graph(int K) {
     if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
     cudaGraph_t g;
@@ -646,6 +699,25 @@ int eb_ctx::run_async(int64_t n) {
     }
     int K = graph_steps > 0 ? graph_steps : 64;
     int64_t done = 0;
+    if (persistent && persist_ok && !profile) {
+        if (pops_dirty) {
+            std::vector<PopDev> h;
+            for (auto &p : pops)
+                if (p.kind != KIND_INPUT) h.push_back(p.dev);
+            CK(cudaMemcpyAsync(d_pops, h.data(), sizeof(PopDev) * h.size(), cudaMemcpyHostToDevice, stream));
+            pops_dirty = false;
+        }
+        const int64_t chunk = 1000;
+        while (done < n) {
+            const int k = (int)std::min<int64_t>(chunk, n - done);
+            cudaError_t e = launch_persistent(persist_class, d_pops, pinfo, net, k, persist_grid, stream);
+            if (e != cudaSuccess) { set_error("persistent kernel launch: %s", cudaGetErrorString(e)); return EB_ERR_CUDA; }
+            launches += 1;
+            done += k;
+        }
+        steps_done = k_end;
+        return EB_OK;
+    }
     if (profile) {
         // one graph of all n steps with timestamped kernels (events are reused only
         // after prof_collect, so n bounds the number of events in flight)
@@ -704,6 +776,7 @@ int eb_ctx::sync() {
         }
         if (f & FLAG_RECORD_OVERFLOW) { set_error("spike recording buffer full (drain with eb_get_spikes or raise eb_set_record_capacity)"); return EB_ERR_OVERFLOW; }
         if (f & FLAG_SPIKELIST_OVERFLOW) { set_error("internal spike list overflow"); return EB_ERR_OVERFLOW; }
+        if (f & FLAG_BARRIER_TIMEOUT) { set_error("persistent kernel: grid barrier wait timed out"); return EB_ERR_CUDA; }
     }
     return EB_OK;
 }
@@ -855,12 +928,43 @@ int eb_inject_spikes(eb_ctx *ctx, int64_t n, const float *time_s, const int64_t 
         if (ctx->finalized && ctx->pops[ctx->pop_of[cell[i]]].kind != KIND_INPUT) {
             for (auto &p : ctx->pops) p.dev.may_repeat = 1;
             ctx->graphs_valid = false;
+            ctx->pops_dirty = true;
         }
     }
     std::stable_sort(ctx->pending.begin(), ctx->pending.end(), [](const PendingIn &a, const PendingIn &b) {
         if (a.t != b.t) return a.t < b.t;
         return a.seq < b.seq;
     });
+    return EB_OK;
+}
+
+int eb_set_timeline(eb_ctx *ctx, int steps) {
+    if (!ctx || steps < 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (!ctx->persist_ok) { set_error("persistent kernel not in use"); return EB_ERR_STATE; }
+    if (steps > 0) {
+        int rc = ctx->dalloc((void **)&ctx->pinfo.tl, sizeof(unsigned long long) * (size_t)steps * 6 * ctx->persist_grid);
+        if (rc) return rc;
+    } else {
+        ctx->pinfo.tl = nullptr;
+    }
+    ctx->pinfo.tl_steps = steps;
+    return EB_OK;
+}
+
+int eb_get_timeline(eb_ctx *ctx, int *grid, unsigned long long *out) {
+    if (!ctx || !grid) { set_error("bad argument"); return EB_ERR_ARG; }
+    *grid = ctx->persist_grid;
+    if (out && ctx->pinfo.tl) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        CK(cudaMemcpy(out, ctx->pinfo.tl, sizeof(unsigned long long) * (size_t)ctx->pinfo.tl_steps * 6 * ctx->persist_grid,
+                      cudaMemcpyDeviceToHost));
+    }
+    return EB_OK;
+}
+
+int eb_set_persistent(eb_ctx *ctx, int on) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    ctx->persistent = on != 0;
     return EB_OK;
 }
 

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "eb_types.h"
+#include "eb_kernels.h"
 
 namespace eb {
 
@@ -62,6 +63,13 @@ struct eb_ctx {
     bool has_inputs = false;
     bool inputs_concurrent = false;  // input fan-out can overlap the neuron updates
     int input_threads = 32;
+    // persistent multi-step kernel
+    bool persistent = false;        // opt-in (eb_set_persistent): grid barriers cost more than launches here
+    bool persist_ok = false;        // set at finalize
+    int persist_class = 0, persist_grid = 0;
+    eb::PersistInfo pinfo{};
+    eb::PopDev *d_pops = nullptr;
+    bool pops_dirty = true;
     // side streams and events for the parallel branches of a step
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> fork_ev, join_ev;
@@ -120,6 +128,7 @@ struct eb_ctx {
     void prof_end(int kind, int pop, cudaEvent_t a);
     int prof_collect();
     int build_graph(int K);
+    int setup_persistent();
     int run_async(int64_t n);
     int sync();
     int snapshot(int slot);

@@ -17,6 +17,7 @@ constexpr uint32_t FLAG_BUCKET_OVERFLOW = 1u;
 constexpr uint32_t FLAG_BDF_SINGULAR = 2u;
 constexpr uint32_t FLAG_RECORD_OVERFLOW = 4u;
 constexpr uint32_t FLAG_SPIKELIST_OVERFLOW = 8u;
+constexpr uint32_t FLAG_BARRIER_TIMEOUT = 16u;
 
 // One delivery waiting in a target's bucket: the arrival time (double seconds,
 // as the reference computes it) and the synapse, both in source-major order

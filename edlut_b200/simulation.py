@@ -32,7 +32,8 @@ class Simulation:
     """
 
     def __init__(self, device: int = 0, record_capacity: Optional[int] = None,
-                 graph_steps: int = 0, bucket_limit: int = 0, input_multiplicity: int = 0):
+                 graph_steps: int = 0, bucket_limit: int = 0, input_multiplicity: int = 0,
+                 persistent: bool = False):
         L = load()
         h = ctypes.c_void_p()
         check(L.eb_ctx_create(device, None, ctypes.byref(h)))
@@ -45,6 +46,7 @@ class Simulation:
             check(L.eb_set_record_capacity(h, int(record_capacity)))
         if graph_steps:
             check(L.eb_set_graph_steps(h, int(graph_steps)))
+        check(L.eb_set_persistent(h, 1 if persistent else 0))
         if bucket_limit or input_multiplicity:
             check(L.eb_set_bucket_limit(h, int(bucket_limit), int(input_multiplicity)))
 

@@ -114,6 +114,19 @@ int eb_load_input_file(eb_ctx *ctx, const char *input_file);
  * TimeDrivenInternalSpike / PropagatedSpikeGroup cycle. */
 int eb_run(eb_ctx *ctx, int64_t n_steps);
 int eb_set_graph_steps(eb_ctx *ctx, int graph_steps);
+/* on != 0: run all phases of up to 1000 steps in one cooperative persistent
+ * kernel with bounded grid barriers where the device and network allow (<= 16
+ * model populations).  0 (default): per-step kernels replayed as CUDA graphs,
+ * which is faster on B200 for the networks measured (a grid barrier over all
+ * SMs costs more than the launches it replaces). */
+int eb_set_persistent(eb_ctx *ctx, int on);
+/* Timeline of the persistent kernel for the first `steps` steps of each launch:
+ * globaltimer (ns) per step, per mark (0 start, 1 phase-A barrier arrival,
+ * 2 phase-A barrier exit, 3 phase-B barrier arrival, 4 end of the block's first
+ * phase-A item, 5 number of phase-A items of the block) and per block:
+ * out[(step * 6 + mark) * grid + block]; *grid receives the block count. */
+int eb_set_timeline(eb_ctx *ctx, int steps);
+int eb_get_timeline(eb_ctx *ctx, int *grid, unsigned long long *out);
 /* Enqueue n_steps on the context stream without synchronizing (error flags are
  * checked by the next eb_sync / eb_run). */
 int eb_run_async(eb_ctx *ctx, int64_t n_steps);

@@ -31,8 +31,16 @@ def run_case(name, chunks=None, **kw):
 
 
 def test_graph_and_plain_launches_agree():
-    a, wa = run_case("adex_rk4_stdp", graph_steps=64)
-    b, wb = run_case("adex_rk4_stdp", graph_steps=1)
+    a, wa = run_case("adex_rk4_stdp", graph_steps=64, persistent=False)
+    b, wb = run_case("adex_rk4_stdp", graph_steps=1, persistent=False)
+    np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(wa, wb)
+
+
+@pytest.mark.parametrize("name", ["cereb_small_rk4", "hh_small_bdf2", "lif_coarse_dt", "adex_dense_fanin"])
+def test_persistent_kernel_and_graphs_agree(name):
+    a, wa = run_case(name, persistent=True)
+    b, wb = run_case(name, persistent=False)
     np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(wa, wb)
 

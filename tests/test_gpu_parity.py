@@ -30,11 +30,12 @@ def run_gpu(net, t, c, nsteps, trace, **kw):
     return out
 
 
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "graphs"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_gpu_matches_reference_fixture(name):
+def test_gpu_matches_reference_fixture(name, persistent):
     net, t, c, nsteps, trace = build_case(name)
     g = load_golden(name)
-    r = run_gpu(net, t, c, nsteps, trace)
+    r = run_gpu(net, t, c, nsteps, trace, persistent=persistent)
     ref = spike_pairs(g["spike_step"], g["spike_cell"])
     same, near = spike_match_fraction(ref, r["spikes"])
     assert same >= 0.999 and near == 1.0, (same, near)
