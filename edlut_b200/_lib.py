@@ -74,6 +74,31 @@ SIGNATURES = [
                                                  ctypes.c_void_p]),
     ("eb_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("eb_restore", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    # batched sweep
+    ("eb_sweep_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                        ctypes.c_float, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("eb_sweep_destroy", ctypes.c_int, [ctypes.c_void_p]),
+    ("eb_sweep_set_network", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, c_f32p, ctypes.c_float, ctypes.c_float,
+                                             ctypes.c_float, ctypes.c_float]),
+    ("eb_sweep_set_inputs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, c_f32p, c_i32p]),
+    ("eb_sweep_build", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_float]),
+    ("eb_sweep_reset", ctypes.c_int, [ctypes.c_void_p]),
+    ("eb_sweep_configure", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("eb_sweep_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)]),
+    ("eb_sweep_run", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("eb_sweep_run_async", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("eb_sweep_sync", ctypes.c_int, [ctypes.c_void_p]),
+    ("eb_sweep_get_spikes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, c_i64p, c_i32p,
+                                            c_i32p]),
+    ("eb_sweep_spike_counts", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
+    ("eb_sweep_get_synapses", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, c_i64p, c_i32p,
+                                              c_i32p, c_f32p]),
+    ("eb_sweep_get_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_f32p]),
+    ("eb_sweep_info", ctypes.c_int, [ctypes.c_void_p, c_i64p, c_i64p, c_i64p, ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    ("eb_sweep_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
 ]
 
 _lib = None

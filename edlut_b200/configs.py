@@ -131,6 +131,49 @@ def sweep_sizes(seed: int = 1, n_networks: int = 4096, n_min: int = 500, n_max: 
     return np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_networks)).astype(np.int64)
 
 
+def sweep_networks(seed: int = 1, n_networks: int = 4096, n_min: int = 500, n_max: int = 5000,
+                   t_end: float = 1.0, dt: float = 1e-4, n_inputs: int = 100, rate_hz: float = 10.0,
+                   p: float = 0.1, variation: float = 0.3, base: dict | None = None,
+                   w_exc_max: float = 0.5, w_inh_max: float = 2.0, w_in_max: float = 0.5,
+                   ref_size: int = 1000):
+    """Specifications of the batched parameter sweep: ``n_networks`` independent
+    LIF networks (80% E / 20% I) with sizes log-uniform in [n_min, n_max], each
+    with its own Poisson seed for ``n_inputs`` inputs at ``rate_hz``.
+
+    Per network, with s_x ~ U[1 - variation, 1 + variation]:
+      * g_leak = base g_leak * s_g;
+      * E_leak = v_thr - (v_thr - base E_leak) * s_e -- the variation applies to the
+        leak's 15 mV distance below threshold, so every network stays excitable
+        rather than firing tonically (E_leak above v_thr);
+      * weight scale s_w on every weight range; recurrent ranges are also scaled by
+        ref_size / n so that each neuron's mean recurrent drive matches the
+        1,000-neuron recurrent workload at every size.
+    Returns a list of dicts with keys n, n_exc, n_in, params, p, w_exc_max,
+    w_inh_max, w_in_max, times, cells (cells are input indices 0..n_in-1)."""
+    sizes = sweep_sizes(seed, n_networks, n_min, n_max)
+    rng = np.random.default_rng([seed, 0x5EED])
+    lo, hi = 1.0 - variation, 1.0 + variation
+    s_g = rng.uniform(lo, hi, n_networks)
+    s_e = rng.uniform(lo, hi, n_networks)
+    s_w = rng.uniform(lo, hi, n_networks)
+    b = dict(base or LIF_C1)
+    specs = []
+    for i, n in enumerate(sizes):
+        n = int(n)
+        prm = dict(b)
+        prm["g_leak"] = float(np.float32(b["g_leak"] * s_g[i]))
+        prm["e_leak"] = float(np.float32(b["v_thr"] - (b["v_thr"] - b["e_leak"]) * s_e[i]))
+        rec_scale = s_w[i] * ref_size / n
+        irng = np.random.default_rng([seed, 1, i])
+        times, cells = poisson_input_times(irng, n_inputs, rate_hz, t_end, dt)
+        specs.append(dict(n=n, n_exc=int(round(0.8 * n)), n_in=n_inputs, params=prm, p=p,
+                          w_exc_max=float(np.float32(w_exc_max * rec_scale)),
+                          w_inh_max=float(np.float32(w_inh_max * rec_scale)),
+                          w_in_max=float(np.float32(w_in_max * s_w[i])),
+                          times=times, cells=cells.astype(np.int32)))
+    return specs
+
+
 # Per-model synaptic weight ranges that give moderate firing in parity_network.
 _PARITY_W = {
     "LIFTimeDrivenModel": dict(w_in=0.5, w_exc=0.5, w_inh=2.0),

@@ -209,6 +209,55 @@ int eb_fold_arrivals_noalloc(void *stream, int64_t n, const int32_t *target, con
 int eb_snapshot(eb_ctx *ctx, int slot);
 int eb_restore(eb_ctx *ctx, int slot);
 
+/* ------------------------------------------------------ batched sweep --- */
+/* Many independent LIF networks of uneven size advanced by one persistent kernel
+ * (the parameter-sweep use: the reference runs one Simulation per parameter set,
+ * Simulation::RunSimulation, src/simulation/Simulation.cpp:285-320, each with
+ * its own network file; the reference README describes sweeps of several hundred
+ * million 5k-neuron simulations).  Network i: n LIF neurons (neurons [0, n_exc) excitatory
+ * sources, AMPA; [n_exc, n) inhibitory, GABA) and n_in input neurons (sources
+ * n .. n+n_in-1, AMPA) driven by given spike times; every source connects to
+ * every neuron with probability p through one delay, weights uniform in
+ * [0, w_max) of the source's class, drawn on the device from a hash of (seed,
+ * network, source, target).  Each network's spikes equal a run of the same
+ * network (eb_sweep_get_synapses, LIF layer first, inputs after) on the plain
+ * path.  Up to 65535 networks of at most 16384 neurons; Euler, RK2 or RK4. */
+typedef struct eb_sweep eb_sweep;
+int eb_sweep_create(int device, int n_networks, int integrator, float dt_s, float delay_s, uint64_t seed,
+                    eb_sweep **out);
+int eb_sweep_destroy(eb_sweep *h);
+/* lif_params: the 10 LIFTimeDrivenModel .cfg values in file order
+ * (LIFTimeDrivenModel::ParseNeuronModel, src/neuron_model/LIFTimeDrivenModel.cpp:459-540). */
+int eb_sweep_set_network(eb_sweep *h, int i, int n, int n_in, int n_exc, const float *lif_params, float p,
+                         float w_exc_max, float w_inh_max, float w_in_max);
+/* Input spikes of network i: times in seconds, cells in [0, n_in). */
+int eb_sweep_set_inputs(eb_sweep *h, int i, int64_t n, const float *time_s, const int32_t *cell);
+/* Generate connectivity and allocate everything for up to n_steps_max steps;
+ * the spike record holds max_rate_hz mean firing per network. */
+int eb_sweep_build(eb_sweep *h, int64_t n_steps_max, float max_rate_hz);
+/* Back to step 0 (initial state, empty records). */
+int eb_sweep_reset(eb_sweep *h);
+/* Threads per CTA (128/256/512/1024; neurons per thread follow) and steps per
+ * kernel launch; 0 keeps the current value. */
+int eb_sweep_configure(eb_sweep *h, int block, int steps_per_launch);
+/* Time trial_steps from the initial state for each launch configuration, keep
+ * the fastest, leave the sweep reset. */
+int eb_sweep_autotune(eb_sweep *h, int64_t trial_steps, int *best_block, int *best_spl, float *best_ms);
+/* Advance every network n_steps (whole chunks replay one CUDA graph). */
+int eb_sweep_run(eb_sweep *h, int64_t n_steps);
+int eb_sweep_run_async(eb_sweep *h, int64_t n_steps);
+int eb_sweep_sync(eb_sweep *h);
+/* Spikes of network i as (1-based step, neuron), sorted; size query with cap 0. */
+int eb_sweep_get_spikes(eb_sweep *h, int i, int64_t cap, int64_t *n, int32_t *step, int32_t *cell);
+int eb_sweep_spike_counts(eb_sweep *h, int64_t *counts);
+/* Synapses of network i in delivery order (source, then target). */
+int eb_sweep_get_synapses(eb_sweep *h, int i, int64_t cap, int64_t *m, int32_t *src, int32_t *tgt, float *w);
+/* var 0 V, 1 gAMPA, 2 gGABA of the n neurons of network i. */
+int eb_sweep_get_state(eb_sweep *h, int i, int var, float *out);
+int eb_sweep_info(eb_sweep *h, int64_t *synapses, int64_t *device_bytes, int64_t *events, int *block,
+                  int *steps_per_launch, int *grid);
+int eb_sweep_stream(eb_sweep *h, void **stream);
+
 #ifdef __cplusplus
 }
 #endif
