@@ -111,6 +111,41 @@ def build_workload(seed: int, t_end: float, scale: float = 1.0):
                                     pf_per_purkinje=k, t_end=t_end)
 
 
+def layer_starts(net):
+    """First neuron of each layer, plus the total."""
+    return [int(x) for x in np.cumsum([0] + [l.n for l in net.layers])]
+
+
+def roofline_bytes(net, pop_events, pop_spikes, n_int):
+    """Algorithmic bytes per launch of each profiled kernel, keyed like the profile
+    ("update[granule]", ...), from the events delivered into each population and the
+    spikes of each population over `n_int` integration steps."""
+    src = np.asarray(net.src)
+    tgt = np.asarray(net.tgt)
+    plastic = np.asarray(net.wchange) >= 0
+    starts = layer_starts(net)
+    out = {}
+    for q, l in enumerate(net.layers):
+        in_pop = (tgt >= starts[q]) & (tgt < starts[q + 1])
+        frac_plastic = float(plastic[in_pop].mean()) if in_pop.any() else 0.0
+        if l.model != "InputSpikeNeuronModel":
+            mdl = "AdEx" if "AdEx" in l.model else "HH" if "HH" in l.model else "LIF"
+            unit = BYTES_PER_UNIT[mdl] + (96 if mdl == "HH" and l.integrator == "BDF" else 0)
+            ev = pop_events[q] / n_int
+            out["update[%s]" % l.name] = unit * l.n + EVENT_BYTES * ev * (1.0 + frac_plastic)
+            if frac_plastic > 0:
+                per_neuron = int((in_pop & plastic).sum()) / max(1, l.n)
+                out["post_stdp[%s]" % l.name] = EVENT_BYTES * per_neuron * pop_spikes[q] / n_int
+        # fan-out launched from this population's spikes: 8 B per event it writes
+        from_pop = (src >= starts[q]) & (src < starts[q + 1])
+        if from_pop.any():
+            tq = np.searchsorted(starts, tgt[from_pop], side="right") - 1
+            ev_out = sum(pop_events[t] for t in set(tq.tolist()))
+            key = "input_push[-]" if l.model == "InputSpikeNeuronModel" else "push[%s]" % l.name
+            out[key] = EVENT_BYTES * ev_out / n_int
+    return out
+
+
 # ------------------------------------------------------------- our arm ----
 def run_ours(args):
     import torch
@@ -150,6 +185,7 @@ def run_ours(args):
         sim.run(STEPS_PER_BENCH_STEP)
     sim.spikes()
     c0 = sim.counters()
+    pe0 = [sim.population_events(q) for q in range(len(net.layers))]
     l0 = ctypes.c_int64(0)
     _lib.check(L.eb_launch_count(sim._h, ctypes.byref(l0)))
     if world > 1:
@@ -178,7 +214,10 @@ def run_ours(args):
     updates_rank = n_model * STEPS_PER_BENCH_STEP * K
     events_rank = c1["events"] - c0["events"]
     spikes_rank = c1["spikes"] - c0["spikes"]
-    sim.spikes()
+    pop_events = [sim.population_events(q) - pe0[q] for q in range(len(net.layers))]
+    _, sp_cells = sim.spikes()
+    starts = layer_starts(net)
+    pop_spikes = [int(((sp_cells >= starts[q]) & (sp_cells < starts[q + 1])).sum()) for q in range(len(net.layers))]
 
     # per-kernel durations: the same steps replayed as a graph with event-record
     # nodes around every kernel on the stream it runs on
@@ -227,17 +266,20 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(t.item())
 
-    # roofline of the dominant kernel
+    # roofline: algorithmic bytes of each kernel per launch (neuron state 32 B per
+    # LIF/AdEx update, 48 B per HH update; 8 B per delivered event, +8 B when the
+    # synapse is plastic; post-synaptic STDP 8 B per plastic input synapse of each
+    # spiking neuron), divided by its measured average launch time
     peak, peak_kind = measured_peaks()
+    n_int = STEPS_PER_BENCH_STEP * K
+    alg = roofline_bytes(net, pop_events, pop_spikes, n_int)
+    for p in prof:
+        p["alg_bytes_per_launch"] = alg.get(p["kernel"], 0.0)
+        p["achieved_gbs"] = p["alg_bytes_per_launch"] / (p["avg_us"] * 1e-6) / 1e9
     top = prof[0]
-    pop_name = top["kernel"].split("[")[1].rstrip("]")
-    layer = next((l for l in net.layers if l.name == pop_name), None)
-    if top["kernel"].startswith("update") and layer is not None:
-        mdl = "AdEx" if "AdEx" in layer.model else "HH" if "HH" in layer.model else "LIF"
-        alg_bytes = BYTES_PER_UNIT[mdl] * layer.n
-    else:
-        alg_bytes = EVENT_BYTES * events_rank / (STEPS_PER_BENCH_STEP * K)
-    achieved = alg_bytes / (top["avg_us"] * 1e-6) / 1e9
+    achieved = top["achieved_gbs"]
+    step_bytes = sum(alg.get(p["kernel"], 0.0) for p in prof)
+    step_gbs = step_bytes / (sec / n_int) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tf):
@@ -262,19 +304,102 @@ def run_ours(args):
                 "d2h_bytes_per_step": d2h // K},
         "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "traffic": traffic, "alg_bytes_per_launch": top["alg_bytes_per_launch"],
                      "avg_launch_us": top["avg_us"]},
+        "step_roofline": {"alg_bytes_per_integration_step": step_bytes, "achieved": step_gbs,
+                          "unit": "GB/s", "frac": step_gbs / peak},
         "kernels": prof[:8],
         "gpu_launches": int(l1.value - l0.value),
         "clocks": clk,
         "cpu_baseline": cpu,
     }
     sim.close()
+    if args.sweep_networks > 0:
+        result["sweep"] = run_sweep(args, rank, world)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(result))
+
+
+SWEEP_WORKLOAD = ("batched sweep: independent LIF networks, sizes log-uniform 500-5000, 80/20 E/I, p=0.1, "
+                  "100 Poisson inputs at 10 Hz each (per-network seeds), g_leak x U[0.7,1.3], E_leak 15 mV "
+                  "below threshold x U[0.7,1.3], weight scale x U[0.7,1.3] (recurrent ranges x 1000/N), "
+                  "1 ms delay, RK2 dt 0.1 ms, 1 s")
+
+
+def run_sweep(args, rank, world):
+    """Batched-sweep leg: all networks for 1 s of simulated time in one persistent
+    kernel (graph-replayed chunks, autotuned launch shape), against looping the plain
+    path over a sample of the same networks one at a time; the sampled networks'
+    spikes must be identical in both."""
+    import torch
+    from edlut_b200.configs import sweep_networks
+    from edlut_b200.simulation import Simulation
+    from edlut_b200.sweep import Sweep
+    nsteps = args.sweep_steps
+    specs = sweep_networks(seed=1 + rank, n_networks=args.sweep_networks, t_end=nsteps * DT)
+    sw = Sweep.from_specs(specs, n_steps_max=nsteps)
+    tune = sw.autotune(min(500, nsteps))
+    stream = torch.cuda.ExternalStream(sw.stream())
+    times = []
+    for rep in range(2):
+        sw.reset()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sw.run_async(nsteps)
+        b.record(stream)
+        sw.sync()
+        times.append(a.elapsed_time(b) / 1e3)
+    sec = statistics.mean(times)
+    if world > 1:
+        t = torch.tensor([sec], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        sec = float(t.item())
+    info = sw.info()
+    sizes = np.array([sp["n"] for sp in specs])
+    # plain path, one network at a time, on networks spread over the size range
+    sample = np.argsort(sizes)[np.linspace(0, len(sizes) - 1, args.sweep_sample).astype(int)]
+    plain_s, identical = 0.0, True
+    for i in sample:
+        net, t_in, c_in = sw.solo_description(int(i))
+        sim = Simulation.from_description(net, record_capacity=8 << 20)
+        sim.inject_spikes(t_in, c_in)
+        sp = ctypes_stream(sim)
+        st = torch.cuda.ExternalStream(sp)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        sim.run_async(nsteps)
+        b.record(st)
+        sim.sync()
+        plain_s += a.elapsed_time(b) / 1e3
+        s1, c1 = sim.spikes()
+        s2, c2 = sw.spikes(int(i))
+        identical &= bool(len(s1) == len(s2) and np.array_equal(s1, s2) and np.array_equal(c1, c2))
+        sim.close()
+    plain_nps = len(sample) / plain_s
+    nps = world * len(specs) / sec
+    out = {"workload": SWEEP_WORKLOAD, "networks": len(specs) * world, "steps": nsteps,
+           "neurons": int(sizes.sum()) * world, "synapses": info["synapses"] * world,
+           "ms": 1e3 * sec, "networks_per_s": nps,
+           "neuron_updates_per_s": world * int(sizes.sum()) * nsteps / sec,
+           "syn_events_per_s": world * info["events"] / sec,
+           "plain_loop_networks_per_s": plain_nps, "speedup_vs_plain_loop": nps / world / plain_nps,
+           "plain_loop_sample": int(len(sample)), "identical_spikes_in_sample": identical,
+           "autotune": tune, "device_gb": info["device_bytes"] / 1e9, "timing": "CUDA events, mean of 2 runs"}
+    sw.close()
+    return out
+
+
+def ctypes_stream(sim):
+    import ctypes
+    from edlut_b200 import _lib
+    sp = ctypes.c_void_p()
+    _lib.check(sim._L.eb_stream(sim._h, ctypes.byref(sp)))
+    return sp.value
 
 
 # ------------------------------------------------------- reference arm ----
@@ -385,9 +510,23 @@ def main():
     ap.add_argument("--prof-warm", type=int, default=300)
     ap.add_argument("--prof-run", type=int, default=50)
     ap.add_argument("--graph-steps", type=int, default=1)
+    ap.add_argument("--sweep-networks", type=int, default=4096, help="batched-sweep leg (0: skip)")
+    ap.add_argument("--sweep-steps", type=int, default=10000)
+    ap.add_argument("--sweep-sample", type=int, default=6, help="networks also run alone on the plain path")
+    ap.add_argument("--profile-sweep", action="store_true", help="untimed sweep run for an external profiler")
     args = ap.parse_args()
     if args.profile_run:
         run_for_profiler(args)
+        return
+    if args.profile_sweep:
+        from edlut_b200.configs import sweep_networks
+        from edlut_b200.sweep import Sweep
+        specs = sweep_networks(seed=1, n_networks=args.sweep_networks, t_end=args.sweep_steps * DT)
+        sw = Sweep.from_specs(specs, n_steps_max=args.sweep_steps)
+        sw.configure(block=512, steps_per_launch=args.sweep_steps)
+        sw.run(args.sweep_steps)
+        print(json.dumps({"profile_sweep_networks": len(specs), "steps": args.sweep_steps, **sw.info()}))
+        sw.close()
         return
     if args.warmup < 3:
         args.warmup = 3

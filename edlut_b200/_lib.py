@@ -72,6 +72,7 @@ SIGNATURES = [
                                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p]),
+    ("eb_get_population_events", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_i64p]),
     ("eb_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("eb_restore", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     # batched sweep

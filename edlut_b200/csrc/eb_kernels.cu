@@ -210,7 +210,7 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
     unsigned long long cw = c;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cw += __shfl_down_sync(0xffffffffu, cw, o);
-    if ((threadIdx.x & 31) == 0 && cw) atomicAdd(N.events, cw);
+    if ((threadIdx.x & 31) == 0 && cw) atomicAdd(P.events, cw);
     compact_spikes(P, N, k, i, sp);
 }
 
@@ -377,7 +377,7 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
             }
             for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, r[a], x);
         }
-        if (tid == 0) atomicAdd(N.events, (unsigned long long)c);
+        if (tid == 0) atomicAdd(P.events, (unsigned long long)c);
     }
     if (tid == 0) {
         const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x);

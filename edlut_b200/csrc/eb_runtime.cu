@@ -262,8 +262,8 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
     N.expt_aux = exp_table_aux();
     if ((rc = dalloc((void **)&N.flags, sizeof(uint32_t)))) return rc;
     CK(cudaMemsetAsync(N.flags, 0, sizeof(uint32_t), st));
-    if ((rc = dalloc((void **)&N.events, sizeof(unsigned long long)))) return rc;
-    CK(cudaMemsetAsync(N.events, 0, sizeof(unsigned long long), st));
+    if ((rc = dalloc((void **)&N.events, sizeof(unsigned long long) * pops.size()))) return rc;
+    CK(cudaMemsetAsync(N.events, 0, sizeof(unsigned long long) * pops.size(), st));
     if ((rc = dalloc((void **)&N.rec_count, sizeof(unsigned long long)))) return rc;
     CK(cudaMemsetAsync(N.rec_count, 0, sizeof(unsigned long long), st));
     N.rec_cap = rec_cap;
@@ -296,6 +296,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         D.ndiff = model_nd(p.kind);
         D.nvars = model_nv(p.kind);
         D.en = p.en;
+        D.events = N.events + (&p - pops.data());
         D.first = p.first;
         D.n = p.n;
         for (size_t j = 0; j < p.params.size(); ++j) D.p[j] = p.params[j];
@@ -390,7 +391,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
     dyn.push_back({net.pre, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
     dyn.push_back({net.post, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
     dyn.push_back({net.last, sizeof(double) * (size_t)std::max<int64_t>(m, 1)});
-    dyn.push_back({net.events, sizeof(unsigned long long)});
+    dyn.push_back({net.events, sizeof(unsigned long long) * pops.size()});
     for (auto &p : pops) {
         if (p.kind == KIND_INPUT) continue;
         for (int v = 0; v < p.dev.nvars; ++v)
@@ -1107,12 +1108,26 @@ int eb_set_weights(eb_ctx *ctx, const float *w) {
     return EB_OK;
 }
 
+int eb_get_population_events(eb_ctx *ctx, int pop, int64_t *events) {
+    if (!ctx || !events) { set_error("null argument"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    if (pop < 0 || pop >= (int)ctx->pops.size()) { set_error("population %d out of range", pop); return EB_ERR_ARG; }
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long ev = 0;
+    CK(cudaMemcpy(&ev, ctx->net.events + pop, sizeof(ev), cudaMemcpyDeviceToHost));
+    *events = (int64_t)ev;
+    return EB_OK;
+}
+
 int eb_get_counters(eb_ctx *ctx, int64_t *steps, int64_t *spikes, int64_t *events) {
     if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
     if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
     CK(cudaStreamSynchronize(ctx->stream));
-    unsigned long long ev = 0, rc = 0;
-    CK(cudaMemcpy(&ev, ctx->net.events, sizeof(ev), cudaMemcpyDeviceToHost));
+    unsigned long long rc = 0;
+    std::vector<unsigned long long> pe(ctx->pops.size());
+    CK(cudaMemcpy(pe.data(), ctx->net.events, sizeof(unsigned long long) * pe.size(), cudaMemcpyDeviceToHost));
+    unsigned long long ev = 0;
+    for (auto v : pe) ev += v;
     CK(cudaMemcpy(&rc, ctx->net.rec_count, sizeof(rc), cudaMemcpyDeviceToHost));
     if (steps) *steps = ctx->steps_done;
     if (spikes) *spikes = ctx->spikes_drained + (int64_t)rc;

@@ -56,6 +56,7 @@ struct PopDev {
     // in-synapse ranges (target-major) for neurons of this population
     int wide;            // 1: block-per-neuron update (large in-degree)
     int may_repeat;      // a synapse may deliver twice in one step (input-neuron sources)
+    unsigned long long *events;  // delivered synaptic events into this population
 };
 
 // Network-wide device pointers, passed by value to the kernels.
@@ -99,7 +100,7 @@ struct NetDev {
     int64_t rec_cap;
     float *trace;                // [steps][n][kMaxVars]
     int64_t trace_first, trace_n, trace_k0, trace_steps;
-    unsigned long long *events;  // delivered synaptic events
+    unsigned long long *events;  // delivered synaptic events, one counter per population
     uint32_t *flags;
 };
 

@@ -185,6 +185,12 @@ class Simulation:
         check(self._L.eb_get_counters(self._h, ctypes.byref(s), ctypes.byref(sp), ctypes.byref(ev)))
         return dict(steps=s.value, spikes=sp.value, events=ev.value)
 
+    def population_events(self, pop: int) -> int:
+        """Synaptic events delivered into population ``pop`` (layer index)."""
+        e = ctypes.c_int64(0)
+        check(self._L.eb_get_population_events(self._h, int(pop), ctypes.byref(e)))
+        return e.value
+
     def device_bytes(self) -> int:
         b = ctypes.c_int64(0)
         check(self._L.eb_device_bytes(self._h, ctypes.byref(b)))

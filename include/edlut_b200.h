@@ -155,6 +155,8 @@ int eb_get_weights(eb_ctx *ctx, float *w);
 int eb_set_weights(eb_ctx *ctx, const float *w);
 /* Steps done, spikes emitted, synaptic events delivered. */
 int eb_get_counters(eb_ctx *ctx, int64_t *steps, int64_t *spikes, int64_t *events);
+/* Synaptic events delivered into population `pop` (index in eb_add_population order). */
+int eb_get_population_events(eb_ctx *ctx, int pop, int64_t *events);
 /* Device memory held by the context, bytes. */
 int eb_device_bytes(eb_ctx *ctx, int64_t *bytes);
 
