@@ -316,6 +316,8 @@ def run_ours(args):
     sim.close()
     if args.sweep_networks > 0:
         result["sweep"] = run_sweep(args, rank, world)
+    if args.adjoint_networks > 0:
+        result["adjoint"] = run_adjoint(args, rank, world)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -391,6 +393,75 @@ def run_sweep(args, rank, world):
            "plain_loop_sample": int(len(sample)), "identical_spikes_in_sample": identical,
            "autotune": tune, "device_gb": info["device_bytes"] / 1e9, "timing": "CUDA events, mean of 2 runs"}
     sw.close()
+    return out
+
+
+ADJOINT_WORKLOAD = ("adjoint fitting: LIF networks of 10k neurons (80/20 E/I, in-degree exactly 100 recurrent + 10 "
+                    "from 100 Poisson inputs at 10 Hz), RK2 dt 0.1 ms, 5,000 steps, checkpoints every 100 steps; "
+                    "loss = MSE of the V traces of 256 observed neurons per network against traces from hidden "
+                    "ground-truth g_leak/E_leak/tau_AMPA/tau_GABA (x U[0.7,1.3]); gradients for those four "
+                    "parameters per network and every weight")
+
+
+def run_adjoint(args, rank, world):
+    """Adjoint leg: forward (the method's own time stepping, trace of the observed
+    neurons) and forward + backward (adjoint kernel, one recomputation per
+    checkpoint segment) on the fitting workload, timed with CUDA events."""
+    import torch
+    from edlut_b200.adjoint import TraceModel
+    from edlut_b200.configs import adjoint_networks, perturbed_params
+    B, n, steps, every = args.adjoint_networks, args.adjoint_neurons, args.adjoint_steps, 100
+    specs = adjoint_networks(seed=7 + rank, n_networks=B, n=n, t_end=steps * DT)
+    obs = np.stack([np.random.default_rng([7, i]).choice(n, 256, replace=False) for i in range(B)])
+    model = TraceModel(specs, steps, obs, integrator="RK2", checkpoint_every=every)
+    rng = np.random.default_rng(99)
+    truth = np.array([[perturbed_params(s["params"], rng)[k] for k in ("g_leak", "e_leak", "tau_exc", "tau_inh")]
+                      for s in specs])
+    w0 = model.initial_weights()
+    with torch.no_grad():
+        target = model(torch.tensor(truth), w0).clone()
+    params = model.initial_params().requires_grad_()
+    weights = w0.clone().requires_grad_()
+
+    def fwd_only():
+        with torch.no_grad():
+            return model(params, weights)
+
+    def fwd_bwd():
+        params.grad = None
+        weights.grad = None
+        loss = ((model(params, weights) - target) ** 2).mean()
+        loss.backward()
+        return loss
+
+    def timed(fn, reps=2):
+        out = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            out.append(a.elapsed_time(b) / 1e3)
+        return min(out)
+    fwd_only()
+    fwd_bwd()
+    t_f = timed(fwd_only)
+    t_fb = timed(fwd_bwd)
+    loss = float(fwd_bwd().detach())
+    gp = params.grad.numpy()
+    gw = weights.grad
+    info = model.sweep.info()
+    out = {"workload": ADJOINT_WORKLOAD, "networks": B, "neurons_per_network": n, "steps": steps,
+           "checkpoint_every": every, "observed_per_network": 256, "weights": int(model.n_weights),
+           "forward_ms": 1e3 * t_f, "forward_backward_ms": 1e3 * t_fb, "cost_ratio": t_fb / t_f,
+           "backward_over_forward": (t_fb - t_f) / t_f, "loss": loss,
+           "grad_params_norm": float(np.linalg.norm(gp)), "grad_w_norm": float(torch.linalg.norm(gw)),
+           "neuron_updates_per_s_forward": B * n * steps / t_f, "device_gb": info["device_bytes"] / 1e9,
+           "timing": "CUDA events around the whole call (host parameter upload, forward kernels, trace copy; "
+                     "backward adds recompute + adjoint kernels), best of 2"}
+    model.sweep.close()
     return out
 
 
@@ -514,6 +585,9 @@ def main():
     ap.add_argument("--sweep-steps", type=int, default=10000)
     ap.add_argument("--sweep-sample", type=int, default=6, help="networks also run alone on the plain path")
     ap.add_argument("--profile-sweep", action="store_true", help="untimed sweep run for an external profiler")
+    ap.add_argument("--adjoint-networks", type=int, default=64, help="adjoint leg (0: skip)")
+    ap.add_argument("--adjoint-neurons", type=int, default=10000)
+    ap.add_argument("--adjoint-steps", type=int, default=5000)
     args = ap.parse_args()
     if args.profile_run:
         run_for_profiler(args)

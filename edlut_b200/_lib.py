@@ -100,6 +100,16 @@ SIGNATURES = [
     ("eb_sweep_info", ctypes.c_int, [ctypes.c_void_p, c_i64p, c_i64p, c_i64p, ctypes.POINTER(ctypes.c_int),
                                       ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("eb_sweep_stream", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("eb_sweep_set_synapses", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, c_i32p, c_i32p,
+                                              c_f32p]),
+    ("eb_sweep_set_params", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_f32p]),
+    ("eb_sweep_set_weights", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    ("eb_sweep_get_weights", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    ("eb_sweep_set_observed", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_i32p]),
+    ("eb_sweep_get_trace", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]),
+    ("eb_sweep_set_checkpoints", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("eb_sweep_adjoint", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                         ctypes.c_int, c_f64p]),
 ]
 
 _lib = None

@@ -214,3 +214,83 @@ def parity_network(model: str = "LIFTimeDrivenModel", integrator: str = "Euler",
     net.add_synapses(s + pop.start, t + pop.start, d, inh.astype(np.int32), ww, wmax, rule)
     times, cells = poisson_input_times(rng, n_inputs, rate_hz, t_end, dt)
     return net, times, cells + inp.start
+
+
+# Parameters the adjoint differentiates, in the order of its gradient rows.
+ADJOINT_PARAMS = ("g_leak", "e_leak", "tau_exc", "tau_inh")
+
+
+def adjoint_networks(seed: int = 1, n_networks: int = 64, n: int = 10_000, indeg: int = 100,
+                     n_inputs: int = 100, in_indeg: int = 10, rate_hz: float = 10.0, t_end: float = 0.5,
+                     dt: float = 1e-4, w_exc_max: float = 0.5, w_inh_max: float = 2.0,
+                     w_in_max: float = 0.5, base: dict | None = None, tau_exc: float | None = None):
+    """Networks of the adjoint-fitting workload: ``n_networks`` LIF networks of ``n``
+    neurons (80% E / 20% I), each neuron with exactly ``indeg`` recurrent inputs drawn
+    without replacement (the 1,000-neuron recurrent workload's in-degree, so its weight
+    ranges carry over) and ``in_indeg`` inputs from ``n_inputs`` Poisson sources at
+    ``rate_hz`` (per-network seeds).  Parameters are the recurrent workload's (AMPA
+    tau 0.5 ms; ``tau_exc`` overrides it -- longer AMPA time constants at this drive
+    make the explicit integrators unstable at C_m = 2).  Returns specs
+    for :meth:`edlut_b200.sweep.Sweep.from_specs` with explicit ``src``, ``tgt``, ``w``
+    (sources 0..n-1 recurrent, n.. inputs)."""
+    b = dict(base or LIF_C1)
+    if tau_exc is not None:
+        b["tau_exc"] = tau_exc
+    specs = []
+    n_exc = int(round(0.8 * n))
+    for i in range(n_networks):
+        rng = np.random.default_rng([seed, 2, i])
+        # recurrent: per target `indeg` distinct sources
+        src_r = _distinct_rows(rng, n, n, indeg)
+        tgt_r = np.repeat(np.arange(n), indeg)
+        src_r = src_r.reshape(-1)
+        inh = (src_r >= n_exc)
+        w_r = rng.random(len(src_r)) * np.where(inh, w_inh_max, w_exc_max)
+        src_i = _distinct_rows(rng, n, n_inputs, in_indeg).reshape(-1) + n
+        tgt_i = np.repeat(np.arange(n), in_indeg)
+        w_i = rng.random(len(src_i)) * w_in_max
+        times, cells = poisson_input_times(rng, n_inputs, rate_hz, t_end, dt)
+        specs.append(dict(n=n, n_exc=n_exc, n_in=n_inputs, params=dict(b),
+                          src=np.concatenate([src_r, src_i]).astype(np.int32),
+                          tgt=np.concatenate([tgt_r, tgt_i]).astype(np.int32),
+                          w=np.concatenate([w_r, w_i]).astype(np.float32),
+                          times=times, cells=cells.astype(np.int32)))
+    return specs
+
+
+def _distinct_rows(rng, rows: int, n: int, k: int) -> np.ndarray:
+    """rows x k draws without replacement from range(n): the first k distinct values of
+    an i.i.d. stream per row (a uniform random subset), vectorised."""
+    out = np.empty((rows, k), np.int64)
+    todo = np.arange(rows)
+    extra = 8 + k // 4
+    while len(todo):
+        m = k + extra
+        draw = rng.integers(0, n, size=(len(todo), m))
+        order = np.argsort(draw, axis=1, kind="stable")
+        srt = np.take_along_axis(draw, order, 1)
+        first = np.ones_like(srt, bool)
+        first[:, 1:] = srt[:, 1:] != srt[:, :-1]
+        keep = np.empty_like(first)
+        np.put_along_axis(keep, order, first, 1)
+        ok = keep.sum(1) >= k
+        rank = np.cumsum(keep, 1)
+        sel = keep & (rank <= k)
+        good = todo[ok]
+        out[good] = draw[ok][sel[ok]].reshape(-1, k)
+        todo = todo[~ok]
+        extra *= 2
+    return out
+
+
+def perturbed_params(base: dict, rng, spread: float = 0.3):
+    """A parameter set with each of ADJOINT_PARAMS scaled by U[1 - spread, 1 + spread]
+    (E_leak through its distance below threshold, which keeps it below v_thr)."""
+    p = dict(base)
+    for k in ADJOINT_PARAMS:
+        s = rng.uniform(1 - spread, 1 + spread)
+        if k == "e_leak":
+            p[k] = float(np.float32(base["v_thr"] - (base["v_thr"] - base["e_leak"]) * s))
+        else:
+            p[k] = float(np.float32(base[k] * s))
+    return p

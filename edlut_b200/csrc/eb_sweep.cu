@@ -39,20 +39,13 @@
 #include <cstring>
 #include <vector>
 
-#include "edlut_b200.h"
-#include "eb_runtime.h"
+#include "eb_sweep.h"
 #include "eb_tables.h"
-#include "eb_types.h"
 
 using namespace eb;
+using namespace ebsw;
 
 namespace {
-
-constexpr int kSweepMaxN = 16384;   // neurons per network
-constexpr int kListCap = 512;       // sources per delivery pass
-constexpr int kBatch = 4;           // synapses per thread per delivery batch
-constexpr int kMaxGroups = 3;       // source steps arriving in one step
-constexpr int kMaxFrac = 4;         // steps with a partial refractory fraction
 
 __host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     uint64_t z = x + 0x9E3779B97F4A7C15ull;
@@ -71,63 +64,11 @@ __device__ __forceinline__ bool syn_draw(uint64_t key, int src, int tgt, double 
     return (double)(h >> 11) * (1.0 / 9007199254740992.0) < p;
 }
 
-// LIF parameters and refractory classes of one network.
-struct SweepLif {
-    float e_exc, e_inh, e_leak, v_thr, g_leak, inv_c_m;
-    float decay[2];         // AMPA, GABA decay factors per (half) step
-    int en;                 // bit0 AMPA, bit1 GABA conductances enabled
-    int r_free;             // refr >= r_free (or < 0): no refractory scaling
-    int r_frac0;            // r_frac0 <= refr < r_free: derivative x frac[refr - r_frac0]
-    float frac[kMaxFrac];   // refr < r_frac0: derivative 0
-};
-
-struct SweepNet {
-    int32_t n, n_in, n_exc, wn;   // wn = bitmask words = ceil(n / 32)
-    float p;
-    float w_max[3];               // uniform weight range: excitatory, inhibitory, input sources
-    int64_t src_off;              // into optr (n + n_in + 1 entries, relative offsets)
-    int64_t syn_off;              // first synapse
-    int64_t state_off;            // into V / refr / gE / gI
-    int64_t in_off, n_in_spikes;  // into in_key / in_src
-    int64_t ring_off;             // R * wn words
-    int64_t sum_off;              // R * ceil(wn / 32) words
-    int64_t rec_off, rec_cap;     // into rec (uint16 neurons)
-    float params[10];             // LIF .cfg order
-    SweepLif L;
-};
-
-struct SweepDev {
-    const SweepNet *nets;
-    int n_nets;
-    const int32_t *order;      // network processing order (largest first)
-    int R;                     // delay-ring slots
-    int steps_max;
-    const int32_t *grp_lo;     // [k] first source step arriving at step k
-    const int8_t *grp_n;       // [k] number of source steps arriving at step k
-    const uint32_t *optr;      // per source: synapse offset relative to syn_off
-    const uint16_t *tgt;
-    const float *w;
-    float *V, *gE, *gI;
-    int32_t *refr;
-    uint32_t *ring, *rsum;     // saved bitmask ring and summaries
-    const int32_t *in_key;     // arrival step * 4 + phase, sorted per network
-    const uint16_t *in_src;    // input neuron (local)
-    int64_t *in_cursor;        // per network
-    uint16_t *rec;             // recorded neurons, step-major
-    int32_t *rec_end;          // [net][step-1] record count after the step
-    uint32_t *rec_cnt;         // per network
-    unsigned long long *events;  // per network delivered synaptic events
-    uint32_t *flags;
-    int *queue;
-    int64_t *step;             // steps completed
-    float dt_ms;
-    int integ;
-};
-
 // ------------------------------------------------------- connectivity build --
 // Synapse counts per source: blockIdx.y = network.
 __global__ void k_sweep_count(const SweepNet *nets, uint64_t seed, uint32_t *counts) {
     const SweepNet &S = nets[blockIdx.y];
+    if (S.explicit_syn) return;
     const uint64_t key = net_key(seed, blockIdx.y);
     const int nsrc = S.n + S.n_in;
     __shared__ int sc[32];
@@ -152,6 +93,7 @@ __global__ void k_sweep_count(const SweepNet *nets, uint64_t seed, uint32_t *cou
 // One warp per source writes its targets in increasing order with their weights.
 __global__ void k_sweep_fill(const SweepNet *nets, const uint32_t *optr, uint64_t seed, uint16_t *tgt, float *w) {
     const SweepNet &S = nets[blockIdx.y];
+    if (S.explicit_syn) return;
     const uint64_t key = net_key(seed, blockIdx.y);
     const int nsrc = S.n + S.n_in;
     const int lane = threadIdx.x & 31;
@@ -177,23 +119,6 @@ __global__ void k_sweep_fill(const SweepNet *nets, const uint32_t *optr, uint64_
 }
 
 // --------------------------------------------------------------- neuron update --
-// Derivative of V (lif_deriv of the plain path) with the refractory test given as
-// a class: 0 none, 1 frozen (derivative 0), 2 scaled by f.
-__device__ __forceinline__ float sw_deriv(const SweepLif &L, float V, float gE, float gI, int cls, float f) {
-    if (cls == 1) return 0.0f;
-    float current = 0.0f;
-    if (L.en & 1) current += gE * (L.e_exc - V);
-    if (L.en & 2) current += gI * (L.e_inh - V);
-    const float full = (current + L.g_leak * (L.e_leak - V)) * L.inv_c_m;
-    return cls == 2 ? f * full : full;
-}
-
-__device__ __forceinline__ void sw_decay(const SweepLif &L, float &gE, float &gI) {
-    const float limit = 1e-9;
-    if (L.en & 1) { if (gE < limit) gE = 0.0f; else gE *= L.decay[0]; }
-    if (L.en & 2) { if (gI < limit) gI = 0.0f; else gI *= L.decay[1]; }
-}
-
 // One integration step, operation for operation the plain path's integrate<LIF, INTEG>.
 template <int INTEG>
 __device__ __forceinline__ void sw_integrate(const SweepLif &L, float dt, float &V, float &gE, float &gI, int cls, float f) {
@@ -254,9 +179,9 @@ struct ListGen {
     int32_t nsrc;
 };
 
-template <int INTEG>
+template <int INTEG, bool TRAJ>
 __device__ void sweep_network(const SweepDev &G, const SweepSmem &M, const SweepNet &S, const SweepLif &L, int net,
-                              int64_t k0, int nsteps, int wc, int swc) {
+                              int64_t k0, int nsteps, int wc, int swc, int64_t traj_k0) {
     __shared__ int s_S, s_more;
     __shared__ uint32_t s_rec_n;
     const int n = S.n, n_exc = S.n_exc;
@@ -429,15 +354,22 @@ __device__ void sweep_network(const SweepDev &G, const SweepSmem &M, const Sweep
                 if (i < n) {
                     float v = M.V[i], gE = M.gE[i], gI = M.gI[i];
                     int rr = M.rf[i];
-                    int cls = 0;
+                    int cls = 0, fi = 0;
                     float f = 1.0f;
                     if (rr >= 0 && rr < L.r_free) {
-                        if (rr >= L.r_frac0) { cls = 2; f = L.frac[rr - L.r_frac0]; }
+                        if (rr >= L.r_frac0) { cls = 2; fi = rr - L.r_frac0; f = L.frac[fi]; }
                         else cls = 1;
+                    }
+                    if (TRAJ) {
+                        const int64_t x = (k - traj_k0 - 1) * G.n_total + so + i;
+                        G.tV[x] = v;
+                        G.tE[x] = gE;
+                        G.tI[x] = gI;
                     }
                     sw_integrate<INTEG>(L, dt, v, gE, gI, cls, f);
                     if (rr >= 0) rr++;
                     if (v > L.v_thr) { v = L.e_leak; sp = true; rr = 0; }
+                    if (TRAJ) G.tcode[(k - traj_k0 - 1) * G.n_total + so + i] = (uint8_t)(cls | (fi << 2) | (sp ? kCodeSpike : 0));
                     if (v != v) { v = L.e_leak; gE = 0.0f; gI = 0.0f; }
                     M.V[i] = v;
                     M.rf[i] = rr;
@@ -470,6 +402,9 @@ __device__ void sweep_network(const SweepDev &G, const SweepSmem &M, const Sweep
             for (int a = 0; a < swc; ++a) M.sum[ns * swc + a] = 0u;
         }
         __syncthreads();
+        // observed membrane potentials after step k
+        for (int m = tid; m < G.n_obs; m += nt)
+            G.trace[((int64_t)net * G.steps_max + (k - 1)) * G.n_obs + m] = M.V[G.obs[(int64_t)net * G.n_obs + m]];
     }
     // save the network's state
     for (int i = tid; i < n; i += nt) {
@@ -495,8 +430,8 @@ __device__ void sweep_network(const SweepDev &G, const SweepSmem &M, const Sweep
     __syncthreads();
 }
 
-template <int INTEG>
-__global__ void __launch_bounds__(1024) k_sweep(SweepDev G, int nsteps, int max_n, int wc, int swc) {
+template <int INTEG, bool TRAJ>
+__global__ void __launch_bounds__(1024) k_sweep(SweepDev G, int nsteps, int max_n, int wc, int swc, int64_t traj_k0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SweepSmem M;
     M.V = reinterpret_cast<float *>(smem_raw);
@@ -526,7 +461,7 @@ __global__ void __launch_bounds__(1024) k_sweep(SweepDev G, int nsteps, int max_
         __syncthreads();
         if (threadIdx.x == 0) s_L = s_desc.L;
         __syncthreads();
-        sweep_network<INTEG>(G, M, s_desc, s_L, net, k0, nsteps, wc, swc);
+        sweep_network<INTEG, TRAJ>(G, M, s_desc, s_L, net, k0, nsteps, wc, swc, traj_k0);
     }
 }
 
@@ -539,82 +474,91 @@ __global__ void k_sweep_advance(int64_t *step, int *queue, int nsteps) {
 }  // namespace
 
 // ------------------------------------------------------------------- host --
-struct eb_sweep {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    int n_nets = 0;
-    int integ = INTEG_RK2;
-    float dt = 1e-4f;
-    float delay = 1e-3f;
-    uint64_t seed = 1;
-    std::vector<SweepNet> nets;
-    std::vector<std::vector<float>> in_time;
-    std::vector<std::vector<int32_t>> in_cell;
-    SweepDev G{};
-    std::vector<void *> allocs;
-    std::vector<float> v_init;
-    int64_t steps_done = 0;
-    int64_t total_syn = 0, dev_bytes = 0, state_n = 0, ring_words = 0, sum_words = 0;
-    int max_n = 0;
-    int block = 512, npt = 0, wc = 0, swc = 0;
-    int steps_per_launch = 1000;
-    int grid = 0;
-    size_t smem = 0;
-    cudaGraphExec_t graph = nullptr;
-    int graph_chunks = 0;
-    bool built = false;
-    ~eb_sweep() {
-        if (graph) cudaGraphExecDestroy(graph);
-        for (void *p : allocs) cudaFree(p);
-        if (stream) cudaStreamDestroy(stream);
-    }
-    int dalloc(void **p, size_t b) {
-        if (!b) b = 16;
-        cudaError_t e = cudaMalloc(p, b);
-        if (e != cudaSuccess) { set_error("cudaMalloc(%zu): %s", b, cudaGetErrorString(e)); return EB_ERR_NOMEM; }
-        allocs.push_back(*p);
-        dev_bytes += (int64_t)b;
-        return EB_OK;
-    }
-    int upload(void **d, const void *src, size_t b) {
-        int r = dalloc(d, b);
-        if (r) return r;
-        if (b && src) {
-            cudaError_t e = cudaMemcpy(*d, src, b, cudaMemcpyHostToDevice);
-            if (e != cudaSuccess) { set_error("upload: %s", cudaGetErrorString(e)); return EB_ERR_CUDA; }
-        }
-        return EB_OK;
-    }
-};
-
-#define SK(call)                                                                            \
-    do {                                                                                    \
-        cudaError_t e_ = (call);                                                            \
-        if (e_ != cudaSuccess) {                                                            \
-            set_error("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
-            return EB_ERR_CUDA;                                                             \
-        }                                                                                   \
-    } while (0)
-
 namespace {
 
-using SweepFn = void (*)(SweepDev, int, int, int, int);
+using SweepFn = void (*)(SweepDev, int, int, int, int, int64_t);
 
-SweepFn sweep_fn(int integ) {
+SweepFn sweep_fn(int integ, bool traj) {
     switch (integ) {
-    case INTEG_EULER: return k_sweep<INTEG_EULER>;
-    case INTEG_RK2: return k_sweep<INTEG_RK2>;
-    default: return k_sweep<INTEG_RK4>;
+    case INTEG_EULER: return traj ? k_sweep<INTEG_EULER, true> : k_sweep<INTEG_EULER, false>;
+    case INTEG_RK2: return traj ? k_sweep<INTEG_RK2, true> : k_sweep<INTEG_RK2, false>;
+    default: return traj ? k_sweep<INTEG_RK4, true> : k_sweep<INTEG_RK4, false>;
     }
 }
 
-int enqueue_chunk(eb_sweep *h, int nsteps, cudaStream_t st) {
-    SweepFn f = sweep_fn(h->integ);
-    f<<<h->grid, h->block, h->smem, st>>>(h->G, nsteps, h->max_n, h->wc, h->swc);
+}  // namespace
+
+namespace ebsw {
+
+int enqueue_chunk(eb_sweep *h, int nsteps, cudaStream_t st, bool traj, int64_t traj_k0) {
+    SweepFn f = sweep_fn(h->integ, traj);
+    f<<<h->grid, h->block, h->smem, st>>>(h->G, nsteps, h->max_n, h->wc, h->swc, traj_k0);
     k_sweep_advance<<<1, 1, 0, st>>>(h->G.step, h->G.queue, nsteps);
     SK(cudaGetLastError());
     return EB_OK;
 }
+
+// The arrays that make up the dynamic state, in checkpoint order.
+static void state_arrays(eb_sweep *h, void **ptr, size_t *bytes) {
+    const size_t nt = (size_t)h->state_n, B = (size_t)h->n_nets;
+    void *p[9] = {h->G.V, h->G.gE, h->G.gI, h->G.refr, h->G.ring, h->G.rsum, h->G.in_cursor, h->G.rec_cnt, h->G.events};
+    size_t b[9] = {4 * nt, 4 * nt, 4 * nt, 4 * nt, 4 * (size_t)h->ring_words, 4 * (size_t)h->sum_words, 8 * B, 4 * B, 8 * B};
+    for (int i = 0; i < 9; ++i) { ptr[i] = p[i]; bytes[i] = (b[i] + 255) / 256 * 256; }
+    for (int i = 0; i < 9; ++i) bytes[i] = b[i] ? bytes[i] : 0;
+}
+
+size_t checkpoint_bytes(eb_sweep *h) {
+    void *p[9];
+    size_t b[9], t = 0;
+    state_arrays(h, p, b);
+    for (size_t x : b) t += x;
+    return t;
+}
+
+int checkpoint_save(eb_sweep *h, int c, cudaStream_t st) {
+    void *p[9];
+    size_t b[9], off = 0;
+    state_arrays(h, p, b);
+    unsigned char *dst = (unsigned char *)h->ckpt[c];
+    const size_t real[9] = {4 * (size_t)h->state_n, 4 * (size_t)h->state_n, 4 * (size_t)h->state_n, 4 * (size_t)h->state_n,
+                            4 * (size_t)h->ring_words, 4 * (size_t)h->sum_words, 8 * (size_t)h->n_nets,
+                            4 * (size_t)h->n_nets, 8 * (size_t)h->n_nets};
+    for (int i = 0; i < 9; ++i) {
+        if (real[i]) SK(cudaMemcpyAsync(dst + off, p[i], real[i], cudaMemcpyDeviceToDevice, st));
+        off += b[i];
+    }
+    return EB_OK;
+}
+
+__global__ void k_sweep_set_step(int64_t *step, int *queue, int64_t v) {
+    *step = v;
+    *queue = 0;
+}
+
+int checkpoint_restore(eb_sweep *h, int c, int64_t step, cudaStream_t st) {
+    void *p[9];
+    size_t b[9], off = 0;
+    state_arrays(h, p, b);
+    const unsigned char *src = (const unsigned char *)h->ckpt[c];
+    const size_t real[9] = {4 * (size_t)h->state_n, 4 * (size_t)h->state_n, 4 * (size_t)h->state_n, 4 * (size_t)h->state_n,
+                            4 * (size_t)h->ring_words, 4 * (size_t)h->sum_words, 8 * (size_t)h->n_nets,
+                            4 * (size_t)h->n_nets, 8 * (size_t)h->n_nets};
+    for (int i = 0; i < 9; ++i) {
+        if (real[i]) SK(cudaMemcpyAsync(p[i], src + off, real[i], cudaMemcpyDeviceToDevice, st));
+        off += b[i];
+    }
+    k_sweep_set_step<<<1, 1, 0, st>>>(h->G.step, h->G.queue, step);
+    SK(cudaGetLastError());
+    return EB_OK;
+}
+
+}  // namespace ebsw
+
+namespace {
+
+// LIF parameters of a network from its 10 .cfg values (decay factors and the
+// inverse capacitance computed like the plain path's finalize).
+int fill_lif(eb_sweep *h, const float *lif_params, SweepLif &L);
 
 // Precomputed refractory classes: the plain path's lif_deriv decides per call from
 // l = refr * dt * 1000 (double); here the same comparisons run once per refr value.
@@ -635,6 +579,27 @@ int refractory_classes(float tau_ref, float dt_s, SweepLif &L) {
         if (r > (1 << 24)) return EB_ERR_UNSUPPORTED;
     }
     if (L.r_frac0 < 0) L.r_frac0 = L.r_free;
+    return EB_OK;
+}
+
+int fill_lif(eb_sweep *h, const float *lif_params, SweepLif &L) {
+    const int en = L.en;
+    memset(&L, 0, sizeof(L));
+    L.en = en;
+    L.e_exc = lif_params[0];
+    L.e_inh = lif_params[1];
+    L.e_leak = lif_params[2];
+    L.v_thr = lif_params[3];
+    L.g_leak = lif_params[8];
+    L.inv_c_m = inv_double(lif_params[4]);
+    const float dt_ms = h->dt * 1000.0f;
+    const float el = (h->integ == INTEG_RK4) ? dt_ms * 0.5f : dt_ms;
+    L.decay[0] = decay_factor(el, lif_params[5]);
+    L.decay[1] = decay_factor(el, lif_params[6]);
+    if (refractory_classes(lif_params[7], h->dt, L)) {
+        set_error("refractory period %g ms unsupported at dt %g s", lif_params[7], h->dt);
+        return EB_ERR_UNSUPPORTED;
+    }
     return EB_OK;
 }
 
@@ -660,6 +625,9 @@ int eb_sweep_create(int device, int n_networks, int integrator, float dt_s, floa
     h->nets.resize(n_networks);
     h->in_time.resize(n_networks);
     h->in_cell.resize(n_networks);
+    h->xsrc.resize(n_networks);
+    h->xtgt.resize(n_networks);
+    h->xw.resize(n_networks);
     for (auto &s : h->nets) memset(&s, 0, sizeof(s));
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
@@ -697,22 +665,13 @@ int eb_sweep_set_network(eb_sweep *h, int i, int n, int n_in, int n_exc, const f
     S.w_max[1] = w_inh_max;
     S.w_max[2] = w_in_max;
     for (int j = 0; j < 10; ++j) S.params[j] = lif_params[j];
-    SweepLif &L = S.L;
-    memset(&L, 0, sizeof(L));
-    L.e_exc = lif_params[0];
-    L.e_inh = lif_params[1];
-    L.e_leak = lif_params[2];
-    L.v_thr = lif_params[3];
-    L.g_leak = lif_params[8];
-    L.inv_c_m = inv_double(lif_params[4]);
-    const float dt_ms = h->dt * 1000.0f;
-    const float el = (h->integ == INTEG_RK4) ? dt_ms * 0.5f : dt_ms;
-    L.decay[0] = decay_factor(el, lif_params[5]);
-    L.decay[1] = decay_factor(el, lif_params[6]);
-    if (refractory_classes(lif_params[7], h->dt, L)) {
-        set_error("eb_sweep_set_network: refractory period %g ms unsupported at dt %g s", lif_params[7], h->dt);
-        return EB_ERR_UNSUPPORTED;
-    }
+    S.explicit_syn = 0;
+    h->xsrc[i].clear();
+    h->xtgt[i].clear();
+    h->xw[i].clear();
+    S.L.en = 0;
+    const int rc = fill_lif(h, lif_params, S.L);
+    if (rc) return rc;
     return EB_OK;
 }
 
@@ -726,6 +685,26 @@ int eb_sweep_set_inputs(eb_sweep *h, int i, int64_t n, const float *time_s, cons
         if (!(time_s[q] >= 0.0f)) { set_error("input spike %lld: negative or NaN time", (long long)q); return EB_ERR_ARG; }
     h->in_time[i].assign(time_s, time_s + n);
     h->in_cell[i].assign(cell, cell + n);
+    return EB_OK;
+}
+
+int eb_sweep_set_synapses(eb_sweep *h, int i, int64_t m, const int32_t *src, const int32_t *tgt, const float *w) {
+    if (!h || i < 0 || i >= h->n_nets || m < 0 || (m > 0 && (!src || !tgt || !w))) {
+        set_error("eb_sweep_set_synapses: bad argument");
+        return EB_ERR_ARG;
+    }
+    if (h->built) { set_error("eb_sweep_set_synapses after eb_sweep_build"); return EB_ERR_STATE; }
+    SweepNet &S = h->nets[i];
+    if (S.n <= 0) { set_error("eb_sweep_set_synapses: eb_sweep_set_network(%d) first", i); return EB_ERR_STATE; }
+    for (int64_t k = 0; k < m; ++k)
+        if (src[k] < 0 || src[k] >= S.n + S.n_in || tgt[k] < 0 || tgt[k] >= S.n) {
+            set_error("eb_sweep_set_synapses: synapse %lld out of range", (long long)k);
+            return EB_ERR_ARG;
+        }
+    h->xsrc[i].assign(src, src + m);
+    h->xtgt[i].assign(tgt, tgt + m);
+    h->xw[i].assign(w, w + m);
+    S.explicit_syn = 1;
     return EB_OK;
 }
 
@@ -749,6 +728,7 @@ int eb_sweep_build(eb_sweep *h, int64_t n_steps_max, float max_rate_hz) {
     for (int64_t k = 1; k <= T; ++k) t[k] = t[k - 1] + (double)h->dt;
     std::vector<int32_t> grp_lo(n_steps_max + 2, 0);
     std::vector<int8_t> grp_n(n_steps_max + 2, 0);
+    h->h_arr_step.assign(n_steps_max + 1, INT32_MAX);
     int64_t dmax = 1;
     {
         int64_t ka = 2;
@@ -757,6 +737,7 @@ int eb_sweep_build(eb_sweep *h, int64_t n_steps_max, float max_rate_hz) {
             if (ka < j + 1) ka = j + 1;
             while (ka <= T && t[ka] <= a) ++ka;
             if (ka > n_steps_max) break;
+            h->h_arr_step[j] = (int32_t)ka;
             if (grp_n[ka] == 0) grp_lo[ka] = (int32_t)j;
             if (++grp_n[ka] > kMaxGroups) { set_error("eb_sweep_build: dt too small for the delay grid"); return EB_ERR_UNSUPPORTED; }
             dmax = std::max(dmax, ka - j);
@@ -818,9 +799,12 @@ int eb_sweep_build(eb_sweep *h, int64_t n_steps_max, float max_rate_hz) {
     h->state_n = state_off;
     h->ring_words = ring_off;
     h->sum_words = sum_off;
+    h->h_in_key = in_key;
+    h->G.n_total = state_off;
     int rc;
     SweepNet *d_nets;
     if ((rc = h->upload((void **)&d_nets, h->nets.data(), sizeof(SweepNet) * N))) return rc;
+    h->d_nets = d_nets;
     h->G.nets = d_nets;
     h->G.n_nets = N;
     // connectivity: count per source, scan on the host, fill
@@ -832,6 +816,27 @@ int eb_sweep_build(eb_sweep *h, int64_t n_steps_max, float max_rate_hz) {
     std::vector<uint32_t> cnt(src_off);
     SK(cudaMemcpyAsync(cnt.data(), d_optr, sizeof(uint32_t) * (size_t)src_off, cudaMemcpyDeviceToHost, h->stream));
     SK(cudaStreamSynchronize(h->stream));
+    // explicit networks: synapses sorted by (source, target), the reference's order
+    // for one delay (qsort_inters, src/spike/Network.cpp:45-68), ties by caller order
+    std::vector<std::vector<int64_t>> xord(N);
+    for (int i = 0; i < N; ++i) {
+        if (!h->nets[i].explicit_syn) continue;
+        const SweepNet &S = h->nets[i];
+        auto &o = xord[i];
+        o.resize(h->xsrc[i].size());
+        for (size_t k = 0; k < o.size(); ++k) o[k] = (int64_t)k;
+        const auto &xs = h->xsrc[i], &xt = h->xtgt[i];
+        std::stable_sort(o.begin(), o.end(), [&](int64_t a, int64_t b) {
+            return xs[a] != xs[b] ? xs[a] < xs[b] : xt[a] < xt[b];
+        });
+        for (size_t k = 1; k < o.size(); ++k)
+            if (xs[o[k]] == xs[o[k - 1]] && xt[o[k]] == xt[o[k - 1]]) {
+                set_error("network %d: two synapses from %d to %d (one per pair in a sweep network)", i, xs[o[k]], xt[o[k]]);
+                return EB_ERR_UNSUPPORTED;
+            }
+        for (int s = 0; s < S.n + S.n_in; ++s) cnt[S.src_off + s] = 0;
+        for (size_t k = 0; k < o.size(); ++k) cnt[S.src_off + xs[k]]++;
+    }
     int64_t syn_off = 0;
     for (int i = 0; i < N; ++i) {
         SweepNet &S = h->nets[i];
@@ -861,6 +866,34 @@ int eb_sweep_build(eb_sweep *h, int64_t n_steps_max, float max_rate_hz) {
     h->G.w = d_w;
     k_sweep_fill<<<dim3(64, N), 256, 0, h->stream>>>(d_nets, d_optr, h->seed, d_tgt, d_w);
     SK(cudaGetLastError());
+    // explicit networks' targets and weights, and the sweep -> caller synapse order
+    {
+        std::vector<int64_t> perm(syn_off);
+        std::vector<uint16_t> xt;
+        std::vector<float> xw;
+        for (int i = 0; i < N; ++i) {
+            const SweepNet &S = h->nets[i];
+            const int64_t mi = (i + 1 < N ? h->nets[i + 1].syn_off : syn_off) - S.syn_off;
+            if (!S.explicit_syn) {
+                for (int64_t k = 0; k < mi; ++k) perm[S.syn_off + k] = S.syn_off + k;
+                continue;
+            }
+            const auto &o = xord[i];
+            xt.resize(o.size());
+            xw.resize(o.size());
+            for (size_t k = 0; k < o.size(); ++k) {
+                xt[k] = (uint16_t)h->xtgt[i][o[k]];
+                xw[k] = h->xw[i][o[k]];
+                perm[S.syn_off + (int64_t)k] = S.syn_off + o[k];
+            }
+            if (!o.empty()) {
+                SK(cudaMemcpyAsync(d_tgt + S.syn_off, xt.data(), sizeof(uint16_t) * o.size(), cudaMemcpyHostToDevice, h->stream));
+                SK(cudaMemcpyAsync(d_w + S.syn_off, xw.data(), sizeof(float) * o.size(), cudaMemcpyHostToDevice, h->stream));
+                SK(cudaStreamSynchronize(h->stream));
+            }
+        }
+        if ((rc = h->upload((void **)&h->perm, perm.data(), sizeof(int64_t) * perm.size()))) return rc;
+    }
     // state and tables
     h->v_init.assign(state_off, 0.0f);
     for (int i = 0; i < N; ++i)
@@ -883,6 +916,7 @@ int eb_sweep_build(eb_sweep *h, int64_t n_steps_max, float max_rate_hz) {
     if ((rc = h->upload((void **)&h->G.flags, nullptr, sizeof(uint32_t)))) return rc;
     if ((rc = h->upload((void **)&h->G.queue, nullptr, sizeof(int)))) return rc;
     if ((rc = h->upload((void **)&h->G.step, nullptr, sizeof(int64_t)))) return rc;
+    if ((rc = h->upload((void **)&h->d_arr_step, h->h_arr_step.data(), sizeof(int32_t) * h->h_arr_step.size()))) return rc;
     std::vector<int32_t> order(N);
     for (int i = 0; i < N; ++i) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return h->nets[a].n > h->nets[b].n; });
@@ -913,6 +947,8 @@ int eb_sweep_reset(eb_sweep *h) {
     SK(cudaMemsetAsync(h->G.step, 0, sizeof(int64_t), st));
     SK(cudaStreamSynchronize(st));
     h->steps_done = 0;
+    h->needs_reset = false;
+    h->ckpt_upto = h->ckpt_every > 0 ? 0 : -1;
     return EB_OK;
 }
 
@@ -926,13 +962,16 @@ int eb_sweep_configure(eb_sweep *h, int block, int steps_per_launch) {
     const int swc = (wc + 31) / 32;
     const size_t smem = 16 * (size_t)h->max_n + sizeof(uint32_t) * (size_t)h->G.R * (wc + swc) +
                         sizeof(int32_t) * (3 * (size_t)kListCap + 1);
-    SweepFn f = sweep_fn(h->integ);
+    SweepFn f = sweep_fn(h->integ, false);
     SK(cudaSetDevice(h->device));
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute((const void *)f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) {
-            set_error("sweep kernel: %zu bytes of shared memory unavailable (%s)", smem, cudaGetErrorString(e));
-            return EB_ERR_UNSUPPORTED;
+        for (bool traj : {false, true}) {
+            cudaError_t e = cudaFuncSetAttribute((const void *)sweep_fn(h->integ, traj),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) {
+                set_error("sweep kernel: %zu bytes of shared memory unavailable (%s)", smem, cudaGetErrorString(e));
+                return EB_ERR_UNSUPPORTED;
+            }
         }
     }
     int nsm = 0, occ = 0;
@@ -959,11 +998,30 @@ int eb_sweep_configure(eb_sweep *h, int block, int steps_per_launch) {
 
 int eb_sweep_run_async(eb_sweep *h, int64_t n_steps) {
     if (!h || !h->built) { set_error("eb_sweep_run: sweep not built"); return EB_ERR_STATE; }
+    if (h->needs_reset) { set_error("eb_sweep_run: the adjoint left the sweep mid-run; eb_sweep_reset first"); return EB_ERR_STATE; }
     if (n_steps < 0 || h->steps_done + n_steps > h->G.steps_max) {
         set_error("eb_sweep_run: %lld steps exceed the %d built for", (long long)(h->steps_done + n_steps), h->G.steps_max);
         return EB_ERR_ARG;
     }
     SK(cudaSetDevice(h->device));
+    if (h->ckpt_every > 0) {
+        // chunks aligned to the checkpoint interval, the state saved before each
+        const int E = h->ckpt_every;
+        if (h->steps_done % E) { set_error("eb_sweep_run: checkpointed runs start at a multiple of %d steps", E); return EB_ERR_STATE; }
+        const bool from0 = h->ckpt_upto == h->steps_done;
+        int64_t done = 0;
+        while (done < n_steps) {
+            const int64_t k = h->steps_done + done;
+            const int len = (int)std::min<int64_t>(E, n_steps - done);
+            int rc = checkpoint_save(h, (int)(k / E), h->stream);
+            if (!rc) rc = enqueue_chunk(h, len, h->stream);
+            if (rc) return rc;
+            done += len;
+        }
+        h->steps_done += n_steps;
+        h->ckpt_upto = from0 ? h->steps_done : -1;
+        return EB_OK;
+    }
     const int spl = h->steps_per_launch;
     const int chunks = (int)(n_steps / spl);
     if (chunks > 0) {
@@ -1155,6 +1213,124 @@ int eb_sweep_info(eb_sweep *h, int64_t *synapses, int64_t *device_bytes, int64_t
 int eb_sweep_stream(eb_sweep *h, void **stream) {
     if (!h || !stream) { set_error("eb_sweep_stream: bad argument"); return EB_ERR_ARG; }
     *stream = (void *)h->stream;
+    return EB_OK;
+}
+
+int eb_sweep_set_params(eb_sweep *h, int i, const float *lif_params) {
+    if (!h || i < 0 || i >= h->n_nets || !lif_params || h->nets[i].n <= 0) { set_error("eb_sweep_set_params: bad argument"); return EB_ERR_ARG; }
+    SweepNet &S = h->nets[i];
+    SweepLif L = S.L;
+    int rc = fill_lif(h, lif_params, L);
+    if (rc) return rc;
+    S.L = L;
+    for (int j = 0; j < 10; ++j) S.params[j] = lif_params[j];
+    if (h->built) {
+        SK(cudaSetDevice(h->device));
+        SK(cudaStreamSynchronize(h->stream));
+        SK(cudaMemcpy(h->d_nets + i, &S, sizeof(SweepNet), cudaMemcpyHostToDevice));
+        for (int j = 0; j < S.n; ++j) h->v_init[S.state_off + j] = L.e_leak;
+    }
+    return EB_OK;
+}
+
+namespace {
+__global__ void k_perm_gather(const int64_t *perm, int64_t m, const float *src, float *dst) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < m; p += (int64_t)gridDim.x * blockDim.x)
+        dst[p] = src[perm[p]];
+}
+__global__ void k_perm_scatter(const int64_t *perm, int64_t m, const float *src, float *dst) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < m; p += (int64_t)gridDim.x * blockDim.x)
+        dst[perm[p]] = src[p];
+}
+}  // namespace
+
+static int weights_io(eb_sweep *h, float *buf, int on_device, int to_sweep) {
+    if (!h || !h->built || !buf) { set_error("eb_sweep weights: sweep not built or null buffer"); return EB_ERR_ARG; }
+    SK(cudaSetDevice(h->device));
+    const int64_t m = h->total_syn;
+    if (!m) return EB_OK;
+    float *dev = buf;
+    float *tmp = nullptr;
+    if (!on_device) {
+        SK(cudaMallocAsync((void **)&tmp, sizeof(float) * m, h->stream));
+        dev = tmp;
+        if (to_sweep) SK(cudaMemcpyAsync(tmp, buf, sizeof(float) * m, cudaMemcpyHostToDevice, h->stream));
+    }
+    float *w = const_cast<float *>(h->G.w);
+    if (to_sweep) k_perm_gather<<<592, 256, 0, h->stream>>>(h->perm, m, dev, w);
+    else k_perm_scatter<<<592, 256, 0, h->stream>>>(h->perm, m, w, dev);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && !on_device && !to_sweep) e = cudaMemcpyAsync(buf, tmp, sizeof(float) * m, cudaMemcpyDeviceToHost, h->stream);
+    if (tmp) cudaFreeAsync(tmp, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { set_error("eb_sweep weights: %s", cudaGetErrorString(e)); return EB_ERR_CUDA; }
+    return EB_OK;
+}
+
+int eb_sweep_set_weights(eb_sweep *h, const float *w, int on_device) {
+    return weights_io(h, const_cast<float *>(w), on_device, 1);
+}
+
+int eb_sweep_get_weights(eb_sweep *h, float *w, int on_device) { return weights_io(h, w, on_device, 0); }
+
+int eb_sweep_set_observed(eb_sweep *h, int m, const int32_t *idx) {
+    if (!h || !h->built || m < 0 || (m > 0 && !idx)) { set_error("eb_sweep_set_observed: sweep not built or bad argument"); return EB_ERR_ARG; }
+    for (int i = 0; i < h->n_nets; ++i)
+        for (int q = 0; q < m; ++q)
+            if (idx[(int64_t)i * m + q] < 0 || idx[(int64_t)i * m + q] >= h->nets[i].n) {
+                set_error("eb_sweep_set_observed: network %d index %d out of range", i, idx[(int64_t)i * m + q]);
+                return EB_ERR_ARG;
+            }
+    if (m <= h->G.n_obs && m > 0) {
+        SK(cudaMemcpy((void *)h->G.obs, idx, sizeof(int32_t) * (size_t)h->n_nets * m, cudaMemcpyHostToDevice));
+    } else if (m > 0) {
+        int rc;
+        int32_t *d_obs;
+        float *d_trace;
+        if ((rc = h->upload((void **)&d_obs, idx, sizeof(int32_t) * (size_t)h->n_nets * m))) return rc;
+        if ((rc = h->dalloc((void **)&d_trace, sizeof(float) * (size_t)h->n_nets * h->G.steps_max * m))) return rc;
+        h->G.obs = d_obs;
+        h->G.trace = d_trace;
+    }
+    h->G.n_obs = m;
+    h->h_obs.assign(idx, idx + (size_t)h->n_nets * m);
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+        h->graph_chunks = 0;
+    }
+    return EB_OK;
+}
+
+int eb_sweep_get_trace(eb_sweep *h, float *out, int on_device) {
+    if (!h || !h->built || !out) { set_error("eb_sweep_get_trace: bad argument"); return EB_ERR_ARG; }
+    const int m = h->G.n_obs;
+    if (!m || !h->steps_done) return EB_OK;
+    SK(cudaSetDevice(h->device));
+    const size_t row = sizeof(float) * (size_t)h->steps_done * m;
+    const size_t pitch = sizeof(float) * (size_t)h->G.steps_max * m;
+    SK(cudaMemcpy2DAsync(out, row, h->G.trace, pitch, row, h->n_nets,
+                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+    SK(cudaStreamSynchronize(h->stream));
+    return EB_OK;
+}
+
+int eb_sweep_set_checkpoints(eb_sweep *h, int every) {
+    if (!h || !h->built || every < 0) { set_error("eb_sweep_set_checkpoints: sweep not built or bad interval"); return EB_ERR_ARG; }
+    if (every == 0) { h->ckpt_every = 0; return EB_OK; }
+    if (every > 255) { set_error("eb_sweep_set_checkpoints: at most 255 steps between checkpoints"); return EB_ERR_ARG; }
+    SK(cudaSetDevice(h->device));
+    const int n = (int)((h->G.steps_max + every - 1) / every);
+    const size_t b = checkpoint_bytes(h);
+    while ((int)h->ckpt.size() < n) {
+        void *p;
+        int rc = h->dalloc(&p, b);
+        if (rc) return rc;
+        h->ckpt.push_back(p);
+    }
+    h->ckpt_every = every;
+    h->n_ckpt = n;
+    h->ckpt_upto = h->steps_done == 0 ? 0 : -1;
     return EB_OK;
 }
 

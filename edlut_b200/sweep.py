@@ -45,6 +45,8 @@ class Sweep:
         self.n_exc = np.zeros(n_networks, np.int64)
         self.params: list = [None] * n_networks
         self.inputs: list = [None] * n_networks
+        self.explicit: list = [None] * n_networks
+        self.n_obs = 0
 
     @classmethod
     def from_specs(cls, specs, n_steps_max: int, integrator: str = "RK2", dt: float = 1e-4,
@@ -53,8 +55,11 @@ class Sweep:
         """Build a sweep from :func:`edlut_b200.configs.sweep_networks` specifications."""
         sw = cls(len(specs), integrator, dt, delay, seed, device)
         for i, s in enumerate(specs):
-            sw.set_network(i, s["n"], s["n_in"], s["n_exc"], s["params"], s["p"], s["w_exc_max"],
-                           s["w_inh_max"], s["w_in_max"])
+            sw.set_network(i, s["n"], s["n_in"], s["n_exc"], s["params"], s.get("p", 0.0),
+                           s.get("w_exc_max", 0.0), s.get("w_inh_max", 0.0), s.get("w_in_max", 0.0))
+            if "src" in s:
+                sw.set_synapses(i, s["src"], s["tgt"], s["w"])
+                sw.explicit[i] = True
             sw.set_inputs(i, s["times"], s["cells"])
         sw.build(n_steps_max, max_rate_hz)
         return sw
@@ -76,6 +81,74 @@ class Sweep:
         c = np.ascontiguousarray(cells, np.int32)
         check(self._L.eb_sweep_set_inputs(self._h, int(i), len(t), _ptr(t, c_f32p), _ptr(c, c_i32p)))
         self.inputs[i] = (t, c)
+
+    def set_synapses(self, i: int, src, tgt, w) -> None:
+        """Explicit connectivity of network i (sources: LIF neurons 0..n-1, then the
+        inputs n..n+n_in-1), weights in this order."""
+        s_ = np.ascontiguousarray(src, np.int32)
+        t_ = np.ascontiguousarray(tgt, np.int32)
+        w_ = np.ascontiguousarray(w, np.float32)
+        check(self._L.eb_sweep_set_synapses(self._h, int(i), len(s_), _ptr(s_, c_i32p), _ptr(t_, c_i32p),
+                                            _ptr(w_, c_f32p)))
+
+    def set_params(self, i: int, params: dict) -> None:
+        """New LIF parameters of network i (after build: from the next launch / reset)."""
+        full = dict(self.params[i])
+        full.update(params)
+        pv = np.array([full[k] for k in MODEL_PARAM_ORDER[_LIF]], np.float32)
+        check(self._L.eb_sweep_set_params(self._h, int(i), _ptr(pv, c_f32p)))
+        self.params[i] = full
+
+    def set_weights(self, w) -> None:
+        """All weights (networks in order, each in its set_synapses order): a numpy
+        array or a CUDA float32 tensor."""
+        if hasattr(w, "data_ptr"):
+            check(self._L.eb_sweep_set_weights(self._h, ctypes.c_void_p(w.data_ptr()), 1))
+        else:
+            a = np.ascontiguousarray(w, np.float32)
+            check(self._L.eb_sweep_set_weights(self._h, a.ctypes.data_as(ctypes.c_void_p), 0))
+
+    def get_weights(self) -> np.ndarray:
+        w = np.zeros(max(self.info()["synapses"], 1), np.float32)
+        check(self._L.eb_sweep_get_weights(self._h, w.ctypes.data_as(ctypes.c_void_p), 0))
+        return w[:self.info()["synapses"]]
+
+    def set_observed(self, idx) -> None:
+        """Record V after every step of neurons idx[network][m]."""
+        a = np.ascontiguousarray(idx, np.int32)
+        self.n_obs = a.shape[1] if a.ndim == 2 else 0
+        check(self._L.eb_sweep_set_observed(self._h, int(self.n_obs), _ptr(a.reshape(-1), c_i32p)))
+
+    def trace(self, n_steps: int, out=None):
+        """Observed traces [networks, n_steps, m] (into ``out``, a CUDA tensor, if given)."""
+        if out is not None:
+            check(self._L.eb_sweep_get_trace(self._h, ctypes.c_void_p(out.data_ptr()), 1))
+            return out
+        a = np.zeros((self.n_networks, n_steps, self.n_obs), np.float32)
+        check(self._L.eb_sweep_get_trace(self._h, a.ctypes.data_as(ctypes.c_void_p), 0))
+        return a
+
+    def set_checkpoints(self, every: int) -> None:
+        check(self._L.eb_sweep_set_checkpoints(self._h, int(every)))
+
+    def adjoint(self, grad_trace, grad_w=None):
+        """dL/d(params) [networks, 4] (g_leak, e_leak, tau_exc, tau_inh) and dL/dw for
+        the checkpointed run just made.  grad_trace: numpy [networks, steps, m] or a
+        CUDA tensor; grad_w: a CUDA tensor to fill (else a numpy array is returned)."""
+        gp = np.zeros((self.n_networks, 4), np.float64)
+        if hasattr(grad_trace, "data_ptr"):
+            gt, gt_dev = ctypes.c_void_p(grad_trace.data_ptr()), 1
+        else:
+            g = np.ascontiguousarray(grad_trace, np.float32)
+            gt, gt_dev = g.ctypes.data_as(ctypes.c_void_p), 0
+        if grad_w is not None:
+            check(self._L.eb_sweep_adjoint(self._h, gt, gt_dev, ctypes.c_void_p(grad_w.data_ptr()), 1,
+                                           gp.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+            return gp, grad_w
+        gw = np.zeros(max(self.info()["synapses"], 1), np.float32)
+        check(self._L.eb_sweep_adjoint(self._h, gt, gt_dev, gw.ctypes.data_as(ctypes.c_void_p), 0,
+                                       gp.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return gp, gw[:self.info()["synapses"]]
 
     def build(self, n_steps_max: int, max_rate_hz: float = 200.0) -> None:
         check(self._L.eb_sweep_build(self._h, int(n_steps_max), ctypes.c_float(max_rate_hz)))

@@ -259,6 +259,39 @@ int eb_sweep_get_state(eb_sweep *h, int i, int var, float *out);
 int eb_sweep_info(eb_sweep *h, int64_t *synapses, int64_t *device_bytes, int64_t *events, int *block,
                   int *steps_per_launch, int *grid);
 int eb_sweep_stream(eb_sweep *h, void **stream);
+/* Explicit connectivity of network i (after eb_sweep_set_network, before build):
+ * m synapses source -> target (sources as above, at most one synapse per pair)
+ * with weights, in the caller's order; the network then has no hash synapses. */
+int eb_sweep_set_synapses(eb_sweep *h, int i, int64_t m, const int32_t *src, const int32_t *tgt, const float *w);
+/* New .cfg parameters of network i (before or after build; a built sweep uses
+ * them from its next launch, and the initial V = E_leak from its next reset). */
+int eb_sweep_set_params(eb_sweep *h, int i, const float *lif_params);
+/* All synaptic weights, networks in order, each network's synapses in its
+ * eb_sweep_set_synapses order (hash networks: the delivery order).  w is device
+ * memory when on_device != 0. */
+int eb_sweep_set_weights(eb_sweep *h, const float *w, int on_device);
+int eb_sweep_get_weights(eb_sweep *h, float *w, int on_device);
+/* Record V after every step of m neurons per network (idx[n_networks][m], local
+ * indices); eb_sweep_get_trace copies [n_networks][steps run][m]. */
+int eb_sweep_set_observed(eb_sweep *h, int m, const int32_t *idx);
+int eb_sweep_get_trace(eb_sweep *h, float *out, int on_device);
+/* Save the whole state every `every` (1..255) steps during runs (0: off). */
+int eb_sweep_set_checkpoints(eb_sweep *h, int every);
+
+/* ---------------------------------------------------------------- adjoint --- */
+/* Gradients of a loss L(trace) with respect to every network's g_leak, E_leak,
+ * tau_exc (AMPA), tau_inh (GABA) and every weight, for the run just made from
+ * step 0 with checkpoints (reset, set_checkpoints, run).  grad_trace = dL/dtrace,
+ * [n_networks][steps run][m] (device memory when gt_on_device != 0); grad_w gets
+ * dL/dw in eb_sweep_set_weights order (device memory when gw_on_device != 0);
+ * grad_params gets [n_networks][4] on the host.  Discrete adjoint of the forward
+ * as computed: spike times are the update steps at which V crosses v_thr, so the
+ * threshold crossing enters through the reset V <- E_leak (the adjoint of V is
+ * cut and its value goes to E_leak).  Each segment between checkpoints is
+ * recomputed once.  No counterpart in the reference. Leaves the sweep needing
+ * eb_sweep_reset. */
+int eb_sweep_adjoint(eb_sweep *h, const float *grad_trace, int gt_on_device, float *grad_w, int gw_on_device,
+                     double *grad_params);
 
 #ifdef __cplusplus
 }
