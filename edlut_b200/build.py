@@ -36,20 +36,51 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def _compile_flags():
+    return [*ARCH, "-std=c++17", "-O3", "--fmad=false", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
+            "-diag-suppress", "128", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object (in parallel, one nvcc per file) and link
+    the shared library.  Objects newer than every source and header are reused
+    unless ``force``."""
     if not force and not _stale():
         return OUT
-    os.makedirs(OUT_DIR, exist_ok=True)
+    from concurrent.futures import ThreadPoolExecutor
+    obj_dir = os.path.join(OUT_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(ROOT, "include", "edlut_b200.h"))
+    newest_header = max(os.path.getmtime(h) for h in headers)
+
+    def compile_one(src):
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(obj_dir, src + ".o")
+        if (not force and os.path.exists(obj)
+                and os.path.getmtime(obj) > max(os.path.getmtime(path), newest_header)):
+            return obj, None
+        cmd = [nvcc(), *_compile_flags(), "-c", path, "-o", obj + ".tmp"]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            return obj, "nvcc failed on %s:\n%s%s" % (src, r.stdout[-4000:], r.stderr[-4000:])
+        os.replace(obj + ".tmp", obj)
+        return obj, None
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    errors = [e for _, e in results if e]
+    if errors:
+        raise RuntimeError("\n".join(errors))
     tmp = OUT + ".tmp"
-    cmd = [nvcc(), *ARCH, "-std=c++17", "-O3", "--fmad=false", "-lineinfo",
-           "-Xcompiler", "-fPIC,-ffp-contract=off", "-diag-suppress", "128",
-           "-shared", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
-           *[os.path.join(CSRC, s) for s in SOURCES], "-o", tmp]
+    cmd = [nvcc(), *ARCH, "-shared", *[o for o, _ in results], "-o", tmp]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
+        raise RuntimeError("link failed:\n" + r.stdout[-4000:] + r.stderr[-4000:])
     os.replace(tmp, OUT)
     return OUT
 
