@@ -45,20 +45,22 @@ __device__ __forceinline__ float expt_net(const NetDev &N, float v) {
 }
 
 // STDPWeightChange::ApplyPreSynapticSpike on synapse tp at arrival time a.
-__device__ __forceinline__ void stdp_pre(const NetDev &N, uint32_t tp, int rl, double a) {
-    const float *rp = N.rule_par + rl * 6;
-    float el = (float)(a - N.last[tp]);
-    float pre = N.pre[tp] * expt_net(N, -el * rp[4]);
-    float post = N.post[tp] * expt_net(N, -el * rp[5]);
-    N.last[tp] = a;
+// The record r is the synapse's state as loaded; the updated fields are stored.
+__device__ __forceinline__ void stdp_pre(const NetDev &N, uint32_t tp, const SynRec &r, double a) {
+    const float *rp = N.rule_par + r.rule * 6;
+    float el = (float)(a - r.last);
+    float pre = r.pre * expt_net(N, -el * rp[4]);
+    float post = r.post * expt_net(N, -el * rp[5]);
     pre += 1.0f;
-    float w = N.w[tp];
+    float w = r.w;
     w += -rp[2] * post;
-    float mw = N.maxw[tp];
+    const float mw = r.maxw;
     if (w > mw) w = mw; else if (w < 0.0f) w = 0.0f;
-    N.pre[tp] = pre;
-    N.post[tp] = post;
-    N.w[tp] = w;
+    SynRec *s = N.syn + tp;
+    s->w = w;
+    s->pre = pre;
+    s->post = post;
+    s->last = a;
 }
 
 template <int ND>
@@ -72,9 +74,9 @@ __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
 template <int ND>
 __device__ __forceinline__ void apply_arrival(const NetDev &N, const Arrival &r, float *x) {
     const uint32_t tp = r.tpos;
-    add_conductance<ND>(x, N.stype[tp], N.w[tp]);
-    const int rl = N.rule[tp];
-    if (rl >= 0) stdp_pre(N, tp, rl, r.a);
+    const SynRec s = N.syn[tp];
+    add_conductance<ND>(x, s.stype, s.w);
+    if (s.rule >= 0) stdp_pre(N, tp, s, r.a);
 }
 
 __device__ __forceinline__ int64_t cur_step(const NetDev &N, int rel) { return *N.step + rel + 1; }
@@ -244,26 +246,11 @@ struct WideSmem {
 // STDP pre hook for one arrival with every synapse load issued up front (they
 // only depend on tp); returns the weight before the update through w_old.
 __device__ __forceinline__ void stdp_pre_gather(const NetDev &N, uint32_t tp, double a, float &w_old, int &ty) {
-    const float w = N.w[tp];
-    const int t8 = N.stype[tp];
-    const int rl = N.rule[tp];
-    const double last = N.last[tp];
-    const float pre0 = N.pre[tp], post0 = N.post[tp], mw = N.maxw[tp];
-    w_old = w;
-    ty = t8;
-    if (rl < 0) return;
-    const float *rp = N.rule_par + rl * 6;
-    const float el = (float)(a - last);
-    float pre = pre0 * expt_net(N, -el * rp[4]);
-    float post = post0 * expt_net(N, -el * rp[5]);
-    pre += 1.0f;
-    float wn = w;
-    wn += -rp[2] * post;
-    if (wn > mw) wn = mw; else if (wn < 0.0f) wn = 0.0f;
-    N.last[tp] = a;
-    N.pre[tp] = pre;
-    N.post[tp] = post;
-    N.w[tp] = wn;
+    const SynRec r = N.syn[tp];
+    w_old = r.w;
+    ty = r.stype;
+    if (r.rule < 0) return;
+    stdp_pre(N, tp, r, a);
 }
 
 // Add c weights to the conductances in order.  Each conductance only sees its
@@ -476,21 +463,20 @@ __device__ __forceinline__ void post_item(const PopDev &P, const NetDev &N, int6
     const int64_t t = P.first + P.spk[s];
     const int64_t tp = N.in_ptr[t] + ch * blockDim.x + threadIdx.x;
     if (tp >= N.plastic_end[t]) return;
-    const int rl = N.rule[tp];
-    const float *rp = N.rule_par + rl * 6;
-    const double last = N.last[tp];
-    float pre = N.pre[tp], post = N.post[tp], w = N.w[tp];
-    const float mw = N.maxw[tp];
-    const float el = (float)(tk - last);
+    const SynRec r = N.syn[tp];
+    const float *rp = N.rule_par + r.rule * 6;
+    float pre = r.pre, post = r.post, w = r.w;
+    const float el = (float)(tk - r.last);
     pre *= expt_net(N, -el * rp[4]);
     post *= expt_net(N, -el * rp[5]);
     post += 1.0f;
     w += rp[0] * pre;
-    if (w > mw) w = mw; else if (w < 0.0f) w = 0.0f;
-    N.last[tp] = tk;
-    N.pre[tp] = pre;
-    N.post[tp] = post;
-    N.w[tp] = w;
+    if (w > r.maxw) w = r.maxw; else if (w < 0.0f) w = 0.0f;
+    SynRec *o = N.syn + tp;
+    o->w = w;
+    o->pre = pre;
+    o->post = post;
+    o->last = tk;
 }
 
 __global__ void __launch_bounds__(256) k_push(PopDev P, NetDev N, int rel, double inv_dt) {

@@ -240,16 +240,18 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
     if ((rc = upload(this, (uint16_t **)&N.grp_units, grp_units))) return rc;
     if ((rc = upload(this, (int64_t **)&N.in_ptr, in_ptr))) return rc;
     if ((rc = upload(this, (int64_t **)&N.plastic_end, plastic_end))) return rc;
-    if ((rc = upload(this, &N.w, h_w))) return rc;
-    d_w = N.w;
-    if ((rc = upload(this, (float **)&N.maxw, h_maxw))) return rc;
-    if ((rc = upload(this, (uint8_t **)&N.stype, h_type))) return rc;
-    if ((rc = upload(this, (int8_t **)&N.rule, h_rule))) return rc;
-    std::vector<float> zf(m, 0.0f);
-    std::vector<double> zd(m, 0.0);
-    if ((rc = upload(this, &N.pre, zf))) return rc;
-    if ((rc = upload(this, &N.post, zf))) return rc;
-    if ((rc = upload(this, &N.last, zd))) return rc;
+    {
+        std::vector<SynRec> hs(m);
+        for (int64_t k = 0; k < m; ++k) {
+            SynRec &r = hs[k];
+            memset(&r, 0, sizeof(r));
+            r.w = h_w[k];
+            r.maxw = h_maxw[k];
+            r.stype = h_type[k];
+            r.rule = h_rule[k];
+        }
+        if ((rc = upload(this, &N.syn, hs))) return rc;
+    }
     std::vector<float> rp;
     for (auto &r : rules) {
         rp.push_back(r[0]); rp.push_back(r[1]); rp.push_back(r[2]); rp.push_back(r[3]);
@@ -387,10 +389,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
     dyn.push_back({d_step, sizeof(int64_t)});
     dyn.push_back({net.cnt, sizeof(uint32_t) * (size_t)R * n_neurons});
     dyn.push_back({net.rec, sizeof(Arrival) * (size_t)R * std::max<int64_t>(net.cap_total, 1)});
-    dyn.push_back({net.w, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
-    dyn.push_back({net.pre, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
-    dyn.push_back({net.post, sizeof(float) * (size_t)std::max<int64_t>(m, 1)});
-    dyn.push_back({net.last, sizeof(double) * (size_t)std::max<int64_t>(m, 1)});
+    dyn.push_back({net.syn, sizeof(SynRec) * (size_t)std::max<int64_t>(m, 1)});
     dyn.push_back({net.events, sizeof(unsigned long long) * pops.size()});
     for (auto &p : pops) {
         if (p.kind == KIND_INPUT) continue;
@@ -1091,9 +1090,9 @@ int eb_get_weights(eb_ctx *ctx, float *w) {
     if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
     CK(cudaStreamSynchronize(ctx->stream));
     const int64_t m = (int64_t)ctx->src.size();
-    std::vector<float> h(m);
-    if (m) CK(cudaMemcpy(h.data(), ctx->d_w, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost));
-    for (int64_t k = 0; k < m; ++k) w[k] = h[ctx->tpos_of[k]];
+    std::vector<SynRec> h(m);
+    if (m) CK(cudaMemcpy(h.data(), ctx->net.syn, sizeof(SynRec) * (size_t)m, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < m; ++k) w[k] = h[ctx->tpos_of[k]].w;
     return EB_OK;
 }
 
@@ -1101,10 +1100,11 @@ int eb_set_weights(eb_ctx *ctx, const float *w) {
     if (!ctx || !w) { set_error("bad argument"); return EB_ERR_ARG; }
     if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
     const int64_t m = (int64_t)ctx->src.size();
-    std::vector<float> h(m);
-    for (int64_t k = 0; k < m; ++k) h[ctx->tpos_of[k]] = w[k];
+    std::vector<SynRec> h(m);
     CK(cudaStreamSynchronize(ctx->stream));
-    if (m) CK(cudaMemcpy(ctx->d_w, h.data(), sizeof(float) * (size_t)m, cudaMemcpyHostToDevice));
+    if (m) CK(cudaMemcpy(h.data(), ctx->net.syn, sizeof(SynRec) * (size_t)m, cudaMemcpyDeviceToHost));
+    for (int64_t k = 0; k < m; ++k) h[ctx->tpos_of[k]].w = w[k];
+    if (m) CK(cudaMemcpy(ctx->net.syn, h.data(), sizeof(SynRec) * (size_t)m, cudaMemcpyHostToDevice));
     return EB_OK;
 }
 

@@ -59,7 +59,6 @@ struct eb_ctx {
     std::vector<int64_t> spos_of, tpos_of;
     eb::NetDev net{};
     int64_t *d_step = nullptr;
-    float *d_w = nullptr;
     bool has_inputs = false;
     bool inputs_concurrent = false;  // input fan-out can overlap the neuron updates
     int input_threads = 32;

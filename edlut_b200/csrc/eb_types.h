@@ -29,6 +29,20 @@ struct alignas(16) Arrival {
     uint32_t tpos;
 };
 
+// One synapse in target-major order: everything a delivered spike and the two
+// STDP hooks read or write, in one 32-byte record (one DRAM sector per arrival).
+struct alignas(32) SynRec {
+    float w;        // weight
+    float maxw;     // max weight (clipping of the STDP update)
+    float pre;      // STDP pre-synaptic trace
+    float post;     // STDP post-synaptic trace
+    double last;    // time of the last trace update (s)
+    uint8_t stype;  // 0 AMPA, 1 GABA, 2 NMDA
+    int8_t rule;    // learning rule, -1 none
+    uint8_t pad[6];
+};
+static_assert(sizeof(SynRec) == 32, "SynRec is one sector");
+
 // Per-population parameters, passed by value to the kernels.
 struct PopDev {
     int kind, integ, bdf_order, ndiff, nvars;
@@ -81,12 +95,7 @@ struct NetDev {
     // target-major synapses
     const int64_t *in_ptr;       // [n_neurons+1]
     const int64_t *plastic_end;  // [n_neurons] end of the plastic prefix of each target's range
-    float *w;
-    const float *maxw;
-    const uint8_t *stype;
-    const int8_t *rule;
-    float *pre, *post;
-    double *last;
+    SynRec *syn;                 // [m] target-major synapse records
     const float *rule_par;       // [n_rules][6]: max_LTP, tau_LTP, max_LTD, tau_LTD, inv_LTP, inv_LTD
     const float *exp_table;
     float expt_aux;
