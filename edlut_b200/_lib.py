@@ -16,7 +16,7 @@ EB_OK = 0
 ERRORS = {-1: "EB_ERR_ARG", -2: "EB_ERR_CUDA", -3: "EB_ERR_STATE", -4: "EB_ERR_OVERFLOW",
           -5: "EB_ERR_PARSE", -6: "EB_ERR_UNSUPPORTED", -7: "EB_ERR_NOMEM", -8: "EB_ERR_NUMERIC"}
 KINDS = {"InputSpikeNeuronModel": 0, "LIFTimeDrivenModel": 1, "AdExTimeDrivenModel": 2,
-         "HHTimeDrivenModel": 3}
+         "HHTimeDrivenModel": 3, "PoissonGeneratorDeviceVector": 4}
 INTEGRATORS = {"Euler": 0, "RK2": 1, "RK4": 2, "BDF": 3}
 
 c_i64p = ctypes.POINTER(ctypes.c_int64)
@@ -73,6 +73,8 @@ SIGNATURES = [
                                                  ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
                                                  ctypes.c_void_p]),
     ("eb_get_population_events", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_i64p]),
+    ("eb_set_random_seed", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32]),
+    ("eb_set_poisson_rates", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, c_f32p]),
     ("eb_snapshot", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("eb_restore", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     # batched sweep

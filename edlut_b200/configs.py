@@ -294,3 +294,40 @@ def perturbed_params(base: dict, rng, spread: float = 0.3):
         else:
             p[k] = float(np.float32(base[k] * s))
     return p
+
+
+def poisson_network(seed: int = 1, n: int = 150, generators=((40, 30.0), (30, 80.0)),
+                    after=((20, 30.0),), p: float = 0.2, t_end: float = 0.2, dt: float = 1e-4,
+                    integrator: str = "RK2", stdp: bool = True, w_in: float = 2.0,
+                    w_exc: float = 0.5, w_inh: float = 2.0):
+    """LIF population driven by PoissonGeneratorDeviceVector layers (the device
+    generators replace input-spike lists).  ``generators`` are (size, frequency)
+    layers before the LIF population and ``after`` layers after it; a layer whose
+    frequency equals an earlier one's shares its model type, which decides the order
+    its generators draw their seeds in.  Generator -> LIF synapses are plastic when
+    ``stdp``.  Returns (NetworkDescription, [], [])."""
+    rng = np.random.default_rng(seed)
+    net = NetworkDescription()
+    gens = []
+    for i, (g, f) in enumerate(generators):
+        gens.append(net.add_layer(Layer(g, "PoissonGeneratorDeviceVector", dict(frequency=f),
+                                        name="poisson_%d" % i)))
+    pop = net.add_layer(Layer(n, "LIFTimeDrivenModel", {}, integrator=integrator, dt=dt, name="lif"))
+    for i, (g, f) in enumerate(after):
+        gens.append(net.add_layer(Layer(g, "PoissonGeneratorDeviceVector", dict(frequency=f),
+                                        name="poisson_after_%d" % i)))
+    if stdp:
+        net.rules.append(("STDP", [0.05 * w_in, 0.020, 0.0525 * w_in, 0.020]))
+    for gl in gens:
+        m = rng.random((len(gl), n)) < p
+        s, t = np.nonzero(m)
+        net.add_synapses(s + gl.start, t + pop.start, 1e-3, 0,
+                         (rng.random(len(s)) * w_in).astype(np.float32), w_in, 0 if stdp else -1)
+    n_exc = int(round(0.8 * n))
+    mr = rng.random((n, n)) < 0.1
+    s, t = np.nonzero(mr)
+    inh = s >= n_exc
+    wmax = np.where(inh, w_inh, w_exc).astype(np.float32)
+    net.add_synapses(s + pop.start, t + pop.start, 1e-3, inh.astype(np.int32),
+                     (rng.random(len(s)) * wmax).astype(np.float32), wmax, -1)
+    return net, np.zeros(0, np.float32), np.zeros(0, np.int64)

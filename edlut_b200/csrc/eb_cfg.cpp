@@ -71,13 +71,13 @@ struct RefRandom {
 unsigned long RefRandom::global_seed = 1;
 
 const char *kModelNames[] = {"InputSpikeNeuronModel", "LIFTimeDrivenModel", "AdExTimeDrivenModel",
-                             "HHTimeDrivenModel"};
-const int kModelParams[] = {0, 10, 14, 13};
+                             "HHTimeDrivenModel", "PoissonGeneratorDeviceVector"};
+const int kModelParams[] = {0, 10, 14, 13, 1};
 
 int model_kind(const std::string &name) {
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 5; ++k) {
         std::string n = kModelNames[k];
-        if (name == n || (k > 0 && name == n + "_GPU")) return k;
+        if (name == n || (k > 0 && k < 4 && name == n + "_GPU")) return k;
     }
     return -1;
 }
@@ -92,6 +92,12 @@ int parse_model_cfg(const std::string &path, int kind, std::vector<float> &param
         float v;
         if (std::fscanf(f.fh, "%f", &v) != 1) return f.fail("missing neuron model parameter");
         params.push_back(v);
+    }
+    if (kind == KIND_POISSON) {  // PoissonGeneratorDeviceVector::ParseNeuronModel: the frequency only
+        integ = 0;
+        order = 0;
+        dt = 0.1f / 1000.0f;
+        return EB_OK;
     }
     f.skip_comments();
     char name[65];
@@ -216,7 +222,7 @@ extern "C" int eb_load_network_files(eb_ctx *ctx, const char *network_file, cons
     // weights file
     File g(weights_file);
     if (!g.fh) { set_error("cannot open weights file %s", weights_file); return EB_ERR_PARSE; }
-    RefRandom::global_seed = 1;
+    RefRandom::global_seed = ctx->rng_seed & 0x7fffffffu;
     RefRandom rnd;
     g.skip_comments();
     for (long c = 0; c < ninters;) {

@@ -393,6 +393,29 @@ __global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N
     for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) update_wide_neuron<KIND, INTEG>(P, N, k, i, S);
 }
 
+// PoissonGeneratorDeviceVector::UpdateState (src/neuron_model/PoissonGeneratorDeviceVector.cpp:56-70):
+// a generator with frequency > 0 draws frand() from its own RandomGenerator --
+// x <- (x * 1103515245 + 12345) & 0x7fffffff, frand = (float)x / MAX_RAND
+// (include/simulation/RandomGenerator.h:91-107) -- and fires when
+// frequency * step > frand.  The low 31 bits of the product only depend on its low
+// 32 bits, so 32-bit arithmetic gives the reference's sequence.
+__global__ void __launch_bounds__(256) k_update_poisson(PopDev P, NetDev N, int rel) {
+    const int64_t k = cur_step(N, rel);
+    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool sp = false;
+    if (i < P.n) {
+        const double thr = P.pthr[i];
+        if (thr > 0.0) {
+            const uint32_t x = (P.lcg[i] * 1103515245u + 12345u) & 0x7fffffffu;
+            P.lcg[i] = x;
+            const float r = (float)x / (float)2147483647;
+            sp = thr > (double)r;
+        }
+    }
+    compact_spikes(P, N, k, i, sp);
+}
+
 // ------------------------------------------------------------ spike fan-out --
 // Arrival step of a delivery at time a: the first update time strictly after a
 // (never below k_lo).  The guess floor(a/dt)+1 is confirmed by two independent
@@ -430,7 +453,7 @@ __device__ __forceinline__ void bucket_put(const NetDev &N, int64_t ka, double a
 // One spike of population P at step k (update time t_k): the block's threads
 // cover the source's out-synapses (sorted by delay, then target).
 __device__ __forceinline__ void push_spike(const PopDev &P, const NetDev &N, int64_t k, int64_t s, double inv_dt) {
-    const double tk = N.tstep[k];
+    const double tk = P.kind == KIND_POISSON ? N.tgen[k] : N.tstep[k];  // generators spike on their own grid
     const int64_t src = P.first + P.spk[s];
     const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
     for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
@@ -782,6 +805,7 @@ void launch_update(const PopDev &P, const NetDev &N, int rel, cudaStream_t st) {
     case KIND_LIF: launch_update_k<KIND_LIF>(P, N, rel, st); break;
     case KIND_ADEX: launch_update_k<KIND_ADEX>(P, N, rel, st); break;
     case KIND_HH: launch_update_k<KIND_HH>(P, N, rel, st); break;
+    case KIND_POISSON: k_update_poisson<<<(unsigned)((P.n + 255) / 256), 256, 0, st>>>(P, N, rel); break;
     default: break;
     }
 }

@@ -43,7 +43,9 @@ namespace {
 
 int model_nv(int kind) { return kind == KIND_LIF ? 4 : kind == KIND_ADEX ? 5 : kind == KIND_HH ? 7 : 0; }
 int model_nd(int kind) { return kind == KIND_LIF ? 1 : kind == KIND_ADEX ? 2 : kind == KIND_HH ? 4 : 0; }
-int model_nparams(int kind) { return kind == KIND_LIF ? 10 : kind == KIND_ADEX ? 14 : kind == KIND_HH ? 13 : 0; }
+int model_nparams(int kind) {
+    return kind == KIND_LIF ? 10 : kind == KIND_ADEX ? 14 : kind == KIND_HH ? 13 : kind == KIND_POISSON ? 1 : 0;
+}
 
 }  // namespace
 
@@ -78,12 +80,19 @@ static int upload(eb_ctx *c, T **dptr, const std::vector<T> &h) {
 int eb_ctx::add_population(int kind, int64_t n, int integ, int bdf_order, float dt, const float *params,
                            int n_params, int64_t *out_first) {
     if (finalized) { set_error("eb_add_population after eb_finalize"); return EB_ERR_STATE; }
-    if (n <= 0 || kind < KIND_INPUT || kind > KIND_HH) { set_error("bad population kind/size"); return EB_ERR_ARG; }
+    if (n <= 0 || kind < KIND_INPUT || kind > KIND_POISSON) { set_error("bad population kind/size"); return EB_ERR_ARG; }
     HostPop p;
     p.kind = kind;
     p.n = n;
     p.first = n_neurons;
-    if (kind != KIND_INPUT) {
+    if (kind == KIND_POISSON) {
+        // PoissonGeneratorDeviceVector: one frequency, sampled every 0.1 ms
+        // (sampling_period 0.1f / time scale 1000, PoissonGeneratorDeviceVector.cpp:26,137)
+        if (n_params != 1 || !params) { set_error("a Poisson generator takes 1 parameter (frequency, Hz)"); return EB_ERR_ARG; }
+        p.params.assign(params, params + 1);
+        p.rates.assign(n, params[0]);
+        p.dt = 0.1f / 1000.0f;
+    } else if (kind != KIND_INPUT) {
         if (integ < INTEG_EULER || integ > INTEG_BDF) { set_error("unsupported integrator %d", integ); return EB_ERR_UNSUPPORTED; }
         if (integ == INTEG_BDF && (bdf_order < 1 || bdf_order > 6)) { set_error("BDF order must be 1..6"); return EB_ERR_ARG; }
         if (!(dt > 0.0f)) { set_error("integration step must be > 0"); return EB_ERR_ARG; }
@@ -103,18 +112,55 @@ int eb_ctx::add_population(int kind, int64_t n, int integ, int bdf_order, float 
     return EB_OK;
 }
 
+// Initial states of the Poisson generators' random generators, in the order the
+// reference constructs them: RandomGenerator::srand(seed) (src/EDLUTKernel.cpp:88),
+// one generator for the weights file (src/spike/Network.cpp:662), then one per
+// generator neuron in Network::InitializeStates (src/spike/Network.cpp:274-283):
+// model types in order of first appearance (layers with equal parameters share a
+// type, Network.cpp:1023-1036), neurons of a type in index order; each takes the
+// global seed, which then advances (include/simulation/RandomGenerator.h:61-68).
+int eb_ctx::seed_generators() {
+    uint32_t g = rng_seed & 0x7fffffffu;
+    auto next = [](uint32_t v) { return (v * 765426813u + 54321u) & 0x7fffffffu; };
+    g = next(g);  // the weights loader's generator
+    std::vector<int> type_first;  // first population of each generator type
+    std::vector<std::vector<size_t>> members;
+    for (size_t q = 0; q < pops.size(); ++q) {
+        if (pops[q].kind != KIND_POISSON) continue;
+        size_t t = 0;
+        while (t < type_first.size() && pops[type_first[t]].params != pops[q].params) ++t;
+        if (t == type_first.size()) { type_first.push_back((int)q); members.emplace_back(); }
+        members[t].push_back(q);
+    }
+    for (auto &mem : members)
+        for (size_t q : mem) {
+            std::vector<uint32_t> st(pops[q].n);
+            for (auto &v : st) { v = g; g = next(g); }
+            CK(cudaMemcpyAsync(pops[q].dev.lcg, st.data(), sizeof(uint32_t) * st.size(), cudaMemcpyHostToDevice, stream));
+            CK(cudaStreamSynchronize(stream));
+        }
+    return EB_OK;
+}
+
 int eb_ctx::finalize(int64_t *out_sorted_perm) {
     if (finalized) { set_error("eb_finalize called twice"); return EB_ERR_STATE; }
     if (n_neurons <= 0) { set_error("no populations"); return EB_ERR_STATE; }
     const int64_t m = (int64_t)src.size();
     // step size shared by all model populations
     dt_f = 0.0f;
-    for (auto &p : pops)
-        if (p.kind != KIND_INPUT) {
+    has_generators = false;
+    for (auto &p : pops) {
+        if (p.kind == KIND_POISSON) has_generators = true;
+        if (p.kind != KIND_INPUT && p.kind != KIND_POISSON) {
             if (dt_f == 0.0f) dt_f = p.dt;
             else if (p.dt != dt_f) { set_error("all model populations must share one integration step"); return EB_ERR_UNSUPPORTED; }
         }
-    if (dt_f == 0.0f) dt_f = 1e-4f;
+    }
+    if (dt_f == 0.0f) dt_f = has_generators ? 0.1f / 1000.0f : 1e-4f;
+    if (has_generators && std::fabs((double)dt_f - (double)(0.1f / 1000.0f)) > 1e-9) {
+        set_error("Poisson generators sample every 0.1 ms; the network's step is %g s", (double)dt_f);
+        return EB_ERR_UNSUPPORTED;
+    }
     dt_s = (double)dt_f;
     pop_of.assign(n_neurons, 0);
     for (size_t q = 0; q < pops.size(); ++q)
@@ -128,7 +174,10 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
             return EB_ERR_ARG;
         }
         HostPop &tp = pops[pop_of[tgt[k]]];
-        if (tp.kind == KIND_INPUT) { set_error("synapse %lld targets an input neuron", (long long)k); return EB_ERR_UNSUPPORTED; }
+        if (tp.kind == KIND_INPUT || tp.kind == KIND_POISSON) {
+            set_error("synapse %lld targets an input neuron", (long long)k);
+            return EB_ERR_UNSUPPORTED;
+        }
         if (stype[k] < 0 || stype[k] > 2) {
             set_error("synapse %lld: type %d (only 0 AMPA, 1 GABA, 2 NMDA spike synapses)", (long long)k, stype[k]);
             return EB_ERR_UNSUPPORTED;
@@ -304,63 +353,72 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         for (size_t j = 0; j < p.params.size(); ++j) D.p[j] = p.params[j];
         D.dt_s = p.dt;
         D.dt_ms = p.dt * 1000.0f;  // IntegrationMethodFast.h:192
-        const float *pr = p.params.data();
-        float tau[3] = {0, 0, 0};
-        float init[kMaxVars] = {0};
-        std::vector<float> nmda;
-        if (p.kind == KIND_LIF) {
-            D.inv_c_m = inv_double(pr[4]);
-            tau[0] = pr[5]; tau[1] = pr[6]; tau[2] = pr[9];
-            init[0] = pr[2];
-            nmda = make_nmda_table(pr[0], pr[1], &D.nmda_aux);
-        } else if (p.kind == KIND_ADEX) {
-            D.inv_c_m = inv_double(pr[10]);
-            D.inv_slope = inv_double(pr[2]);
-            D.inv_tau_w = inv_double(pr[4]);
-            tau[0] = pr[11]; tau[1] = pr[12]; tau[2] = pr[13];
-            init[0] = pr[8];
-            nmda = make_nmda_table(pr[5], pr[6], &D.nmda_aux);
+        if (p.kind == KIND_POISSON) {
+            // threshold (double)frequency * step, step = (double)(0.1f / 1000): the
+            // comparison PoissonGeneratorDeviceVector.cpp:61 makes with frand()
+            std::vector<double> thr(p.n);
+            for (int64_t i = 0; i < p.n; ++i) thr[i] = (double)p.rates[i] * (double)p.dt;
+            if ((rc = upload(this, (double **)&D.pthr, thr))) return rc;
+            if ((rc = dalloc((void **)&D.lcg, sizeof(uint32_t) * (size_t)p.n))) return rc;
         } else {
-            D.inv_c_m = inv_double(pr[4]);
-            tau[0] = pr[6]; tau[1] = pr[7]; tau[2] = pr[8];
-            std::vector<float> hh = make_hh_table(pr[5]);
-            D.hh_aux = hh_table_aux();
-            // HHTimeDrivenModel::InitializeStates (HHTimeDrivenModel.cpp:141-166)
-            int pos = (int)((pr[2] - (-90.0f)) * D.hh_aux);
-            if (pos < 0) pos = 0; else if (pos > kHHTable - 1) pos = kHHTable - 1;
-            const float *v = hh.data() + (size_t)pos * 6;
-            init[0] = pr[2];
-            init[1] = v[0] / (v[0] + v[1]);
-            init[2] = v[2] / (v[2] + v[3]);
-            init[3] = v[4] / (v[4] + v[5]);
-            if ((rc = upload(this, (float **)&D.hh_table, hh))) return rc;
-            nmda = make_nmda_table(pr[0], pr[1], &D.nmda_aux);
-        }
-        if ((rc = upload(this, (float **)&D.nmda_table, nmda))) return rc;
-        const float el = (p.integ == INTEG_RK4) ? D.dt_ms * 0.5f : D.dt_ms;  // RK4.h:362
-        for (int c = 0; c < 3; ++c) D.decay[c] = decay_factor(el, tau[c]);
-        bdf_coefficients(D.bdf_coef);
-        memcpy(D.init, init, sizeof(init));
-        D.expt_aux = exp_table_aux();
-        D.exp_table = N.exp_table;
-        const int nd = D.ndiff;
-        for (int v = 0; v < D.nvars; ++v) {
-            bool stored = v < nd || (p.en & (1 << (v - nd)));
-            if (!stored) { D.x[v] = nullptr; continue; }
-            std::vector<float> h(p.n, init[v]);
-            if ((rc = upload(this, &D.x[v], h))) return rc;
-        }
-        if (p.kind == KIND_LIF) {
-            std::vector<int32_t> h(p.n, -1);
-            if ((rc = upload(this, &D.refr, h))) return rc;
-        }
-        if (p.integ == INTEG_BDF) {
-            std::vector<int8_t> hs(p.n, 0);
-            if ((rc = upload(this, &D.bdf_state, hs))) return rc;
-            std::vector<float> hd((size_t)p.bdf_order * nd * p.n, 0.0f);
-            if ((rc = upload(this, &D.bdf_D, hd))) return rc;
-            std::vector<float> hp((size_t)std::max(p.bdf_order - 1, 1) * nd * p.n, 0.0f);
-            if ((rc = upload(this, &D.bdf_P, hp))) return rc;
+            const float *pr = p.params.data();
+            float tau[3] = {0, 0, 0};
+            float init[kMaxVars] = {0};
+            std::vector<float> nmda;
+            if (p.kind == KIND_LIF) {
+                D.inv_c_m = inv_double(pr[4]);
+                tau[0] = pr[5]; tau[1] = pr[6]; tau[2] = pr[9];
+                init[0] = pr[2];
+                nmda = make_nmda_table(pr[0], pr[1], &D.nmda_aux);
+            } else if (p.kind == KIND_ADEX) {
+                D.inv_c_m = inv_double(pr[10]);
+                D.inv_slope = inv_double(pr[2]);
+                D.inv_tau_w = inv_double(pr[4]);
+                tau[0] = pr[11]; tau[1] = pr[12]; tau[2] = pr[13];
+                init[0] = pr[8];
+                nmda = make_nmda_table(pr[5], pr[6], &D.nmda_aux);
+            } else {
+                D.inv_c_m = inv_double(pr[4]);
+                tau[0] = pr[6]; tau[1] = pr[7]; tau[2] = pr[8];
+                std::vector<float> hh = make_hh_table(pr[5]);
+                D.hh_aux = hh_table_aux();
+                // HHTimeDrivenModel::InitializeStates (HHTimeDrivenModel.cpp:141-166)
+                int pos = (int)((pr[2] - (-90.0f)) * D.hh_aux);
+                if (pos < 0) pos = 0; else if (pos > kHHTable - 1) pos = kHHTable - 1;
+                const float *v = hh.data() + (size_t)pos * 6;
+                init[0] = pr[2];
+                init[1] = v[0] / (v[0] + v[1]);
+                init[2] = v[2] / (v[2] + v[3]);
+                init[3] = v[4] / (v[4] + v[5]);
+                if ((rc = upload(this, (float **)&D.hh_table, hh))) return rc;
+                nmda = make_nmda_table(pr[0], pr[1], &D.nmda_aux);
+            }
+            if ((rc = upload(this, (float **)&D.nmda_table, nmda))) return rc;
+            const float el = (p.integ == INTEG_RK4) ? D.dt_ms * 0.5f : D.dt_ms;  // RK4.h:362
+            for (int c = 0; c < 3; ++c) D.decay[c] = decay_factor(el, tau[c]);
+            bdf_coefficients(D.bdf_coef);
+            memcpy(D.init, init, sizeof(init));
+            D.expt_aux = exp_table_aux();
+            D.exp_table = N.exp_table;
+            const int nd = D.ndiff;
+            for (int v = 0; v < D.nvars; ++v) {
+                bool stored = v < nd || (p.en & (1 << (v - nd)));
+                if (!stored) { D.x[v] = nullptr; continue; }
+                std::vector<float> h(p.n, init[v]);
+                if ((rc = upload(this, &D.x[v], h))) return rc;
+            }
+            if (p.kind == KIND_LIF) {
+                std::vector<int32_t> h(p.n, -1);
+                if ((rc = upload(this, &D.refr, h))) return rc;
+            }
+            if (p.integ == INTEG_BDF) {
+                std::vector<int8_t> hs(p.n, 0);
+                if ((rc = upload(this, &D.bdf_state, hs))) return rc;
+                std::vector<float> hd((size_t)p.bdf_order * nd * p.n, 0.0f);
+                if ((rc = upload(this, &D.bdf_D, hd))) return rc;
+                std::vector<float> hp((size_t)std::max(p.bdf_order - 1, 1) * nd * p.n, 0.0f);
+                if ((rc = upload(this, &D.bdf_P, hp))) return rc;
+            }
         }
         if ((rc = dalloc((void **)&D.spk, sizeof(uint32_t) * (size_t)p.n))) return rc;
         if ((rc = dalloc((void **)&D.spk_count, 2 * sizeof(uint32_t)))) return rc;
@@ -384,6 +442,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         p.push_threads = (int)std::min<int64_t>(256, std::max<int64_t>(32, (max_out + 31) / 32 * 32));
         D.may_repeat = in_from_inputs > 0 ? 1 : 0;
     }
+    if ((rc = seed_generators())) return rc;
     // dynamic state copied by eb_snapshot / eb_restore
     dyn.clear();
     dyn.push_back({d_step, sizeof(int64_t)});
@@ -403,6 +462,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
             dyn.push_back({p.dev.bdf_P, sizeof(float) * (size_t)std::max(p.bdf_order - 1, 1) * nd * p.n});
         }
         dyn.push_back({p.dev.spk_count, 2 * sizeof(uint32_t)});
+        if (p.dev.lcg) dyn.push_back({p.dev.lcg, sizeof(uint32_t) * (size_t)p.n});
     }
     for (int q = 0; q < 4; ++q) {
         cudaStream_t ss;
@@ -433,6 +493,20 @@ int eb_ctx::ensure_tables(int64_t kmax) {
         double t = t_host.back() + (double)dt_f;  // TimeEventUpdateNeurons.cpp:115
         t_host.push_back(t);
     }
+    if (has_generators) {
+        // generators keep their own grid, t'_k = t'_{k-1} + (double)(0.1f / 1000); their
+        // k-th draw belongs to step k while t_k <= t'_k < t_{k+1}
+        const double gstep = (double)(0.1f / 1000.0f);
+        while ((int64_t)tgen_host.size() <= kmax) {
+            const int64_t k = (int64_t)tgen_host.size();
+            const double t = tgen_host.back() + gstep;
+            if (k + 1 < (int64_t)t_host.size() && !(t_host[k] <= t && t < t_host[k + 1])) {
+                set_error("Poisson generator step %lld falls outside the network step (grids drifted apart)", (long long)k);
+                return EB_ERR_UNSUPPORTED;
+            }
+            tgen_host.push_back(t);
+        }
+    }
     int64_t need = kmax + 1;
     if (need > tcap) {
         int64_t ncap = std::max<int64_t>(need * 2, 4096);
@@ -441,6 +515,7 @@ int eb_ctx::ensure_tables(int64_t kmax) {
         int rc;
         if ((rc = dalloc((void **)&nt, sizeof(double) * (size_t)ncap))) return rc;
         if ((rc = dalloc((void **)&ni, sizeof(int64_t) * (size_t)(ncap + 1)))) return rc;
+        if (has_generators && (rc = dalloc((void **)&d_tgen, sizeof(double) * (size_t)ncap))) return rc;
         CK(cudaMemsetAsync(ni, 0, sizeof(int64_t) * (size_t)(ncap + 1), stream));
         if (d_instart && tcap > 0)
             CK(cudaMemcpyAsync(ni, d_instart, sizeof(int64_t) * (size_t)(tcap + 1), cudaMemcpyDeviceToDevice, stream));
@@ -453,9 +528,13 @@ int eb_ctx::ensure_tables(int64_t kmax) {
     if (tstep_uploaded < need) {
         CK(cudaMemcpyAsync(d_tstep + tstep_uploaded, t_host.data() + tstep_uploaded,
                            sizeof(double) * (size_t)(need - tstep_uploaded), cudaMemcpyHostToDevice, stream));
+        if (has_generators)
+            CK(cudaMemcpyAsync(d_tgen + tstep_uploaded, tgen_host.data() + tstep_uploaded,
+                               sizeof(double) * (size_t)(need - tstep_uploaded), cudaMemcpyHostToDevice, stream));
         tstep_uploaded = need;
     }
     net.tstep = d_tstep;
+    net.tgen = d_tgen;
     net.in_start = d_instart;
     return EB_OK;
 }
@@ -629,6 +708,7 @@ int eb_ctx::setup_persistent() {
     memset(&pinfo, 0, sizeof(pinfo));
     for (auto &p : pops) {
         if (p.kind == KIND_INPUT) continue;
+        if (p.kind == KIND_POISSON) return EB_OK;  // generators run on the graph path only
         if (n_model < kMaxPersistPops) {
             if (p.has_out) pinfo.has_out |= 1u << n_model;
             if (p.has_plastic_in) pinfo.has_plastic |= 1u << n_model;
@@ -1105,6 +1185,41 @@ int eb_set_weights(eb_ctx *ctx, const float *w) {
     if (m) CK(cudaMemcpy(h.data(), ctx->net.syn, sizeof(SynRec) * (size_t)m, cudaMemcpyDeviceToHost));
     for (int64_t k = 0; k < m; ++k) h[ctx->tpos_of[k]].w = w[k];
     if (m) CK(cudaMemcpy(ctx->net.syn, h.data(), sizeof(SynRec) * (size_t)m, cudaMemcpyHostToDevice));
+    return EB_OK;
+}
+
+int eb_set_random_seed(eb_ctx *ctx, uint32_t seed) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (ctx->finalized) { set_error("eb_set_random_seed after eb_finalize"); return EB_ERR_STATE; }
+    ctx->rng_seed = seed;
+    return EB_OK;
+}
+
+int eb_set_poisson_rates(eb_ctx *ctx, int64_t first, int64_t n, const float *rates_hz) {
+    if (!ctx || n < 0 || (n > 0 && !rates_hz) || first < 0 || first + n > ctx->n_neurons) {
+        set_error("eb_set_poisson_rates: bad argument");
+        return EB_ERR_ARG;
+    }
+    for (auto &p : ctx->pops) {
+        const int64_t lo = std::max(first, p.first), hi = std::min(first + n, p.first + p.n);
+        if (lo >= hi) continue;
+        if (p.kind != KIND_POISSON) {
+            set_error("eb_set_poisson_rates: neurons %lld..%lld are not Poisson generators", (long long)lo, (long long)hi - 1);
+            return EB_ERR_ARG;
+        }
+    }
+    for (auto &p : ctx->pops) {
+        const int64_t lo = std::max(first, p.first), hi = std::min(first + n, p.first + p.n);
+        if (lo >= hi) continue;
+        for (int64_t i = lo; i < hi; ++i) p.rates[i - p.first] = rates_hz[i - first];
+        if (ctx->finalized) {
+            std::vector<double> thr(hi - lo);
+            for (int64_t i = lo; i < hi; ++i) thr[i - lo] = (double)p.rates[i - p.first] * (double)p.dt;
+            CK(cudaStreamSynchronize(ctx->stream));
+            CK(cudaMemcpy(const_cast<double *>(p.dev.pthr) + (lo - p.first), thr.data(), sizeof(double) * thr.size(),
+                          cudaMemcpyHostToDevice));
+        }
+    }
     return EB_OK;
 }
 

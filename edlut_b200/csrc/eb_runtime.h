@@ -26,6 +26,7 @@ struct HostPop {
     bool has_out = false, has_plastic_in = false;
     int post_chunks = 1;
     int push_threads = 32;
+    std::vector<float> rates;   // Poisson generators: per-neuron frequency (Hz)
     PopDev dev{};
 };
 
@@ -49,6 +50,7 @@ struct eb_ctx {
     std::vector<float> delay, weight, max_weight;
     std::vector<int32_t> stype, rule;
     uint32_t bucket_limit = 8192, input_multiplicity = 2;
+    uint32_t rng_seed = 1;  // RandomGenerator::srand value (the reference's EDLUTKernel uses 1)
     int64_t rec_cap = 16 << 20;
     // derived
     bool finalized = false;
@@ -75,6 +77,9 @@ struct eb_ctx {
     // time grid and inputs
     std::vector<double> t_host;
     double *d_tstep = nullptr;
+    double *d_tgen = nullptr;             // generator update times (when there are generators)
+    std::vector<double> tgen_host{0.0};
+    bool has_generators = false;
     int64_t *d_instart = nullptr;
     int64_t tcap = 0, tstep_uploaded = 0;
     std::vector<int64_t> in_start_host;
@@ -128,6 +133,7 @@ struct eb_ctx {
     int prof_collect();
     int build_graph(int K);
     int setup_persistent();
+    int seed_generators();
     int run_async(int64_t n);
     int sync();
     int snapshot(int slot);

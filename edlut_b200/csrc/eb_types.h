@@ -4,7 +4,7 @@
 
 namespace eb {
 
-enum Kind : int { KIND_INPUT = 0, KIND_LIF = 1, KIND_ADEX = 2, KIND_HH = 3 };
+enum Kind : int { KIND_INPUT = 0, KIND_LIF = 1, KIND_ADEX = 2, KIND_HH = 3, KIND_POISSON = 4 };
 enum Integ : int { INTEG_EULER = 0, INTEG_RK2 = 1, INTEG_RK4 = 2, INTEG_BDF = 3 };
 
 constexpr int kMaxVars = 8;
@@ -71,6 +71,9 @@ struct PopDev {
     int wide;            // 1: block-per-neuron update (large in-degree)
     int may_repeat;      // a synapse may deliver twice in one step (input-neuron sources)
     unsigned long long *events;  // delivered synaptic events into this population
+    // Poisson generators: LCG state and firing threshold rate * step per neuron
+    uint32_t *lcg;
+    const double *pthr;
 };
 
 // Network-wide device pointers, passed by value to the kernels.
@@ -79,6 +82,7 @@ struct NetDev {
     int R;                       // delay-ring slots
     const int64_t *step;         // current step counter (steps completed)
     const double *tstep;         // update times t_k, k = 0..
+    const double *tgen;          // Poisson generators' own update times (step 0.1f/1000 s)
     // arrival buckets
     uint32_t *cnt;               // [R][n_neurons]
     Arrival *rec;                // [R][cap_total]

@@ -39,6 +39,8 @@ MODEL_PARAM_ORDER: Dict[str, List[str]] = {
     # src/neuron_model/HHTimeDrivenModel.cpp (ParseNeuronModel)
     "HHTimeDrivenModel": ["e_exc", "e_inh", "e_leak", "g_leak", "c_m", "v_thr", "tau_exc",
                           "tau_inh", "tau_nmda", "g_na", "g_kd", "e_na", "e_k"],
+    # src/neuron_model/PoissonGeneratorDeviceVector.cpp:175-200 (ParseNeuronModel)
+    "PoissonGeneratorDeviceVector": ["frequency"],
 }
 # The *_GPU model names read the same parameter files in the same order.
 for _n in list(MODEL_PARAM_ORDER):
@@ -59,6 +61,8 @@ MODEL_DEFAULTS: Dict[str, Dict[str, float]] = {
     "HHTimeDrivenModel": dict(e_exc=0.0, e_inh=-80.0, e_leak=-65.0, g_leak=10.0, c_m=120.0,
                               v_thr=-52.0, tau_exc=5.0, tau_inh=10.0, tau_nmda=20.0,
                               g_na=20000.0, g_kd=6000.0, e_na=50.0, e_k=-90.0),
+    # PoissonGeneratorDeviceVector::GetDefaultParameters (PoissonGeneratorDeviceVector.cpp:162-167)
+    "PoissonGeneratorDeviceVector": dict(frequency=10.0),
 }
 for _n in list(MODEL_DEFAULTS):
     MODEL_DEFAULTS[_n + "_GPU"] = MODEL_DEFAULTS[_n]
@@ -145,6 +149,8 @@ class NetworkDescription:
             f.write("// %s parameters (one value per line, EDLUT .cfg layout)\n" % base)
             for k in order:
                 f.write("// %s\n%s\n" % (k, _f32(p[k])))
+            if base == "PoissonGeneratorDeviceVector":  # a device: no integration method
+                return
             f.write("// integration method\n%s\n" % layer.integrator)
             if layer.integrator == "BDF":
                 f.write("// BDF order\n%d\n" % layer.bdf_order)

@@ -33,7 +33,7 @@ class Simulation:
 
     def __init__(self, device: int = 0, record_capacity: Optional[int] = None,
                  graph_steps: int = 0, bucket_limit: int = 0, input_multiplicity: int = 0,
-                 persistent: bool = False):
+                 persistent: bool = False, random_seed: Optional[int] = None):
         L = load()
         h = ctypes.c_void_p()
         check(L.eb_ctx_create(device, None, ctypes.byref(h)))
@@ -47,6 +47,8 @@ class Simulation:
         if graph_steps:
             check(L.eb_set_graph_steps(h, int(graph_steps)))
         check(L.eb_set_persistent(h, 1 if persistent else 0))
+        if random_seed is not None:
+            check(L.eb_set_random_seed(h, int(random_seed)))
         if bucket_limit or input_multiplicity:
             check(L.eb_set_bucket_limit(h, int(bucket_limit), int(input_multiplicity)))
 
@@ -118,6 +120,11 @@ class Simulation:
         return self.sorted_perm
 
     # ------------------------------------------------------------- running --
+    def set_poisson_rates(self, first: int, rates_hz) -> None:
+        """Per-neuron frequencies of Poisson generator neurons first, first+1, ..."""
+        r = np.ascontiguousarray(rates_hz, np.float32)
+        check(self._L.eb_set_poisson_rates(self._h, int(first), len(r), _ptr(r, c_f32p)))
+
     def inject_spikes(self, times: Sequence[float], cells: Sequence[int]) -> None:
         t = np.ascontiguousarray(times, np.float32)
         c = np.ascontiguousarray(cells, np.int64)

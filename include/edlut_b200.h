@@ -44,6 +44,10 @@ extern "C" {
 #define EB_LIF 1
 #define EB_ADEX 2
 #define EB_HH 3
+/* PoissonGeneratorDeviceVector (src/neuron_model/PoissonGeneratorDeviceVector.cpp):
+ * params = {frequency in Hz}; it samples every 0.1 ms, so the network's other
+ * populations must use that step. */
+#define EB_POISSON 4
 /* Integration methods "Euler", "RK2", "RK4", "BDF"
  * (src/integration_method/IntegrationMethodFactory_GPU_C_INTERFACE.cu:54-97). */
 #define EB_EULER 0
@@ -155,6 +159,15 @@ int eb_get_weights(eb_ctx *ctx, float *w);
 int eb_set_weights(eb_ctx *ctx, const float *w);
 /* Steps done, spikes emitted, synaptic events delivered. */
 int eb_get_counters(eb_ctx *ctx, int64_t *steps, int64_t *spikes, int64_t *events);
+/* Seed of the reference's random generators (RandomGenerator::srand,
+ * include/simulation/RandomGenerator.h:61-64; EDLUTKernel uses 1, the default).
+ * It fixes the Poisson generators' sequences; call before eb_finalize. */
+int eb_set_random_seed(eb_ctx *ctx, uint32_t seed);
+/* Per-neuron frequencies (Hz) of Poisson generator neurons first .. first+n-1,
+ * the vector parameter PoissonGeneratorDeviceVector::SetSpecificNeuronParameters
+ * sets (src/neuron_model/PoissonGeneratorDeviceVector.cpp:142-155).  Before or
+ * after eb_finalize. */
+int eb_set_poisson_rates(eb_ctx *ctx, int64_t first, int64_t n, const float *rates_hz);
 /* Synaptic events delivered into population `pop` (index in eb_add_population order). */
 int eb_get_population_events(eb_ctx *ctx, int pop, int64_t *events);
 /* Device memory held by the context, bytes. */

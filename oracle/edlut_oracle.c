@@ -34,7 +34,7 @@
 #include <string.h>
 
 #define EO_MAXV 8
-enum { EO_INPUT = 0, EO_LIF = 1, EO_ADEX = 2, EO_HH = 3 };
+enum { EO_INPUT = 0, EO_LIF = 1, EO_ADEX = 2, EO_HH = 3, EO_POISSON = 4 };
 enum { EO_EULER = 0, EO_RK2 = 1, EO_RK4 = 2, EO_BDF = 3 };
 
 /* ExponentialTable constants, include/simulation/ExponentialTable.h / ExponentialTable.cpp */
@@ -70,6 +70,7 @@ typedef struct eo_popstate {
     int *bdf_state;
     void *bdf_D_f32, *bdf_P_f32, *bdf_D_f64, *bdf_P_f64;
     float init[EO_MAXV];
+    uint32_t *rng;              /* Poisson generators: RandomGenerator::next_element per neuron */
 } eo_popstate;
 
 #define R float
@@ -136,6 +137,15 @@ static void init_pop(eo_popstate *ps, const eo_pop *pp, int fp64) {
     ps->dt_ms = pp->dt * 1000.0f; /* IntegrationMethodFast.h:192 */
     const float *p = ps->p;
     float tau[3] = {0, 0, 0};
+    if (ps->kind == EO_POISSON) {
+        /* PoissonGeneratorDeviceVector: sampling period 0.1f ms in a millisecond-scale
+         * model, step = 0.1f / 1000 s (PoissonGeneratorDeviceVector.cpp:26,137) */
+        ps->ndiff = 0; ps->nvars = 0;
+        ps->dt_s = 0.1f / 1000.0f;
+        ps->dt_ms = ps->dt_s * 1000.0f;
+        ps->rng = (uint32_t *)calloc((size_t)ps->n, sizeof(uint32_t));
+        return;
+    }
     if (ps->kind == EO_LIF) {
         ps->ndiff = 1; ps->nvars = 5;
         ps->inv_c_m = (float)(1. / (double)p[4]);
@@ -200,7 +210,7 @@ static void init_pop(eo_popstate *ps, const eo_pop *pp, int fp64) {
 }
 
 static void free_pop(eo_popstate *ps) {
-    free(ps->hh_table); free(ps->bdf_state);
+    free(ps->hh_table); free(ps->bdf_state); free(ps->rng);
     free(ps->bdf_D_f32); free(ps->bdf_P_f32); free(ps->bdf_D_f64); free(ps->bdf_P_f64);
 }
 
@@ -259,6 +269,12 @@ double eo_round_delay(float d) {
     return r <= 0 ? minpd : r;
 }
 
+/* RandomGenerator (include/simulation/RandomGenerator.h:61-107): srand value;
+ * EDLUTKernel calls srand(1) (src/EDLUTKernel.cpp:88). */
+static uint32_t g_seed = 1;
+void eo_set_seed(uint32_t seed) { g_seed = seed & 0x7fffffffu; }
+static uint32_t next_seed(uint32_t g) { return (g * 765426813u + 54321u) & 0x7fffffffu; }
+
 /* Error codes */
 #define EO_OK 0
 #define EO_ERR_ARG -1
@@ -293,6 +309,24 @@ int eo_run(int32_t n_pops, const eo_pop *pops, int64_t n_neurons,
     for (int q = 0; q < n_pops; ++q) {
         init_pop(&ps[q], &pops[q], fp64);
         for (int64_t i = pops[q].first; i < pops[q].first + pops[q].n; ++i) pop_of[i] = q;
+    }
+    /* Generator seeds: one RandomGenerator for the weights file (Network.cpp:662), then
+     * one per generator neuron in Network::InitializeStates: model types (equal
+     * parameters share one, Network.cpp:1023-1036) in order of first appearance, the
+     * neurons of a type in index order (PoissonGeneratorDeviceVector.cpp:96-99). */
+    {
+        uint32_t g = next_seed(g_seed);
+        for (int q = 0; q < n_pops; ++q) {
+            if (ps[q].kind != EO_POISSON) continue;
+            int first_of_type = 1;
+            for (int r = 0; r < q; ++r)
+                if (ps[r].kind == EO_POISSON && ps[r].p[0] == ps[q].p[0]) first_of_type = 0;
+            if (!first_of_type) continue;
+            for (int r = q; r < n_pops; ++r) {
+                if (ps[r].kind != EO_POISSON || ps[r].p[0] != ps[q].p[0]) continue;
+                for (int64_t j = 0; j < ps[r].n; ++j) { ps[r].rng[j] = g; g = next_seed(g); }
+            }
+        }
     }
     /* Synapse types enable the conductances of the target model (CheckSynapseType). */
     for (int64_t k = 0; k < m; ++k) {
@@ -362,7 +396,12 @@ int eo_run(int32_t n_pops, const eo_pop *pops, int64_t n_neurons,
     int64_t nspk = 0, nev = 0;
     double t_now = 0.0;
     float dt_f = 0;
-    for (int q = 0; q < n_pops; ++q) if (ps[q].kind != EO_INPUT) { dt_f = ps[q].dt_s; break; }
+    for (int q = 0; q < n_pops; ++q) if (ps[q].kind != EO_INPUT && ps[q].kind != EO_POISSON) { dt_f = ps[q].dt_s; break; }
+    if (dt_f == 0) dt_f = 0.1f / 1000.0f;
+    /* Poisson generators run on their own grid: TimeEventUpdateNeurons of their model
+     * at t' = t' + (double)(0.1f / 1000) (TimeEventUpdateNeurons.cpp:115); their k-th
+     * update falls between the k-th and (k+1)-th neuron updates for the runs here. */
+    double t_gen = 0.0;
 
     for (int64_t step = 1; step <= nsteps + (tail ? 1 : 0) && rc == EO_OK; ++step) {
         int last_pass = step > nsteps;
@@ -413,18 +452,30 @@ int eo_run(int32_t n_pops, const eo_pop *pops, int64_t n_neurons,
             }
         }
         if (last_pass) break;
+        t_gen += (double)(0.1f / 1000.0f);
         /* 2. neuron updates, 3. spikes (per population, ascending index) */
         for (int q = 0; q < n_pops && rc == EO_OK; ++q) {
             eo_popstate *p = &ps[q];
             if (p->kind == EO_INPUT) continue;
             for (int64_t j = 0; j < p->n; ++j) {
                 int64_t i = p->first + j;
-                int sp = fp64 ? step_neuron_f64(p, j, xd + i * EO_MAXV, &lst[i])
+                int sp;
+                if (p->kind == EO_POISSON) {
+                    /* PoissonGeneratorDeviceVector::UpdateState, PoissonGeneratorDeviceVector.cpp:56-70 */
+                    sp = 0;
+                    if (p->p[0] > 0.0f) {
+                        p->rng[j] = (p->rng[j] * 1103515245u + 12345u) & 0x7fffffffu;
+                        float r = ((float)p->rng[j]) / 2147483647;
+                        sp = (double)p->p[0] * (double)p->dt_s > (double)r;
+                    }
+                } else {
+                    sp = fp64 ? step_neuron_f64(p, j, xd + i * EO_MAXV, &lst[i])
                               : step_neuron_f32(p, j, xf + i * EO_MAXV, &lst[i]);
-                if (sp < 0) { rc = EO_ERR_SINGULAR; break; }
-                /* CheckValidIntegration: reset neurons whose V became NaN */
-                if (fp64 ? isnan(xd[i * EO_MAXV]) : isnan(xf[i * EO_MAXV]))
-                    for (int v = 0; v < EO_MAXV; ++v) { xf[i * EO_MAXV + v] = p->init[v]; xd[i * EO_MAXV + v] = p->init[v]; }
+                    if (sp < 0) { rc = EO_ERR_SINGULAR; break; }
+                    /* CheckValidIntegration: reset neurons whose V became NaN */
+                    if (fp64 ? isnan(xd[i * EO_MAXV]) : isnan(xf[i * EO_MAXV]))
+                        for (int v = 0; v < EO_MAXV; ++v) { xf[i * EO_MAXV + v] = p->init[v]; xd[i * EO_MAXV + v] = p->init[v]; }
+                }
                 if (!sp) continue;
                 if (nspk >= spike_cap) { rc = EO_ERR_SPIKECAP; break; }
                 spike_step[nspk] = step; spike_cell[nspk] = i; nspk++;
@@ -451,8 +502,9 @@ int eo_run(int32_t n_pops, const eo_pop *pops, int64_t n_neurons,
                     }
                 }
                 /* one delivery event per distinct delay at t + d */
+                const double t_spk = p->kind == EO_POISSON ? t_gen : t_now;
                 for (int64_t g = grp_ptr[i]; g < grp_ptr[i + 1]; ++g) {
-                    eo_event e = {t_now + dly[ord[grp_start[g]]], seq++, i, (int32_t)(g - grp_ptr[i]), 0};
+                    eo_event e = {t_spk + dly[ord[grp_start[g]]], seq++, i, (int32_t)(g - grp_ptr[i]), 0};
                     heap_push(&heap, e);
                 }
             }

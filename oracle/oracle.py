@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
 KIND = {"InputSpikeNeuronModel": 0, "LIFTimeDrivenModel": 1, "AdExTimeDrivenModel": 2,
-        "HHTimeDrivenModel": 3}
+        "HHTimeDrivenModel": 3, "PoissonGeneratorDeviceVector": 4}
 INTEG = {"Euler": 0, "RK2": 1, "RK4": 2, "BDF": 3}
 MAXV = 8
 
@@ -46,7 +46,13 @@ def lib():
         _lib.eo_run.restype = ctypes.c_int
         _lib.eo_round_delay.restype = ctypes.c_double
         _lib.eo_round_delay.argtypes = [ctypes.c_float]
+        _lib.eo_set_seed.argtypes = [ctypes.c_uint32]
     return _lib
+
+
+def set_seed(seed: int) -> None:
+    """RandomGenerator::srand value for the Poisson generators (default 1)."""
+    lib().eo_set_seed(int(seed))
 
 
 def _p(a, ct):

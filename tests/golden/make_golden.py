@@ -51,6 +51,10 @@ CASES["cereb_small_rk4"] = ("cerebellar_layer", dict(n_granule=2000, n_mossy=100
                                                      pf_per_purkinje=1000, t_end=0.3),
                             3000, (300, 100, 8))
 CASES["hh_small_bdf2"] = ("hh_network", dict(n=400, indeg=40, t_end=0.1), 2000, (400, 400, 8))
+# device Poisson generators (PoissonGeneratorDeviceVector): two generator types, one
+# of them split around the LIF layer (its seeds follow the first part's), STDP on
+# the generator synapses
+CASES["poisson_lif_rk2_stdp"] = ("poisson_network", dict(seed=6), 2000, (300, 70, 8))
 
 
 def build_case(name: str):
@@ -77,7 +81,8 @@ def make(name: str) -> dict:
     steps = step_of_times(R["spike_time"], dt, nsteps)
     order = np.lexsort((R["spike_cell"], steps))
     nd = {"LIF": 1, "AdE": 2, "HHT": 4}
-    model = next(l.model for l in net.layers if l.model != "InputSpikeNeuronModel")
+    model = next(l.model for l in net.layers
+                 if l.model not in ("InputSpikeNeuronModel", "PoissonGeneratorDeviceVector"))
     out = dict(spike_step=steps[order].astype(np.int32), spike_cell=R["spike_cell"][order].astype(np.int32),
                trace=R["trace"][:, :, :nd[model[:3]]].astype(np.float32),
                counts=np.array(R["counts"], np.int64))

@@ -78,12 +78,14 @@ def test_snapshot_restore_replays_identically():
     np.testing.assert_array_equal(w1, w2)
 
 
-def test_reference_files_load_identically(tmp_path):
+@pytest.mark.parametrize("case", ["lif_rk2_stdp", "poisson_lif_rk2_stdp"])
+def test_reference_files_load_identically(tmp_path, case):
     """eb_load_network_files / eb_load_input_file read the reference's own text
-    formats (network, weights, model .cfg, input spikes) into the same network."""
+    formats (network, weights, model .cfg -- Poisson generator .cfg included --,
+    input spikes) into the same network."""
     from edlut_b200.network import write_input_spikes
     from edlut_b200.simulation import Simulation
-    net, t, c, nsteps, _ = build_case("lif_rk2_stdp")
+    net, t, c, nsteps, _ = build_case(case)
     netf, wf = net.write_files(str(tmp_path))
     inp = os.path.join(str(tmp_path), "inputs.cfg")
     write_input_spikes(inp, t, c)
@@ -99,7 +101,7 @@ def test_reference_files_load_identically(tmp_path):
         sim.close()
     finally:
         os.chdir(cwd)
-    b, wb = run_case("lif_rk2_stdp")
+    b, wb = run_case(case)
     np.testing.assert_array_equal(a, b)
     np.testing.assert_array_equal(wa, wb)
 
