@@ -44,6 +44,24 @@ BYTES_PER_UNIT = {"AdEx": 32, "LIF": 32, "HH": 48}  # algorithmic bytes per neur
 EVENT_BYTES = 8
 
 
+def max_over_ranks(x: float, world: int) -> float:
+    """The slowest rank's value (the job's time): all-reduce MAX over the process
+    group, on the GPU with NCCL, on the CPU with gloo."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Workload seed of a replica: every rank simulates its own networks."""
+    return base + rank
+
+
 def env_rank():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
 
@@ -164,7 +182,7 @@ def run_ours(args):
     prof_steps = 1
     total_bench = W + K + prof_steps + K  # warmup, timed, profiled, e2e
     t_total = (total_bench * STEPS_PER_BENCH_STEP + 10) * DT
-    net, tin, cin = build_workload(seed=1 + rank, t_end=t_total, scale=args.scale)
+    net, tin, cin = build_workload(seed=rank_seed(1, rank), t_end=t_total, scale=args.scale)
     n_model = sum(l.n for l in net.layers if l.model != "InputSpikeNeuronModel")
     sim = Simulation.from_description(net, device=dev, record_capacity=8 << 20)
     L = _lib.load()
@@ -207,10 +225,7 @@ def run_ours(args):
     l1 = ctypes.c_int64(0)
     _lib.check(L.eb_launch_count(sim._h, ctypes.byref(l1)))
     sec = ms / 1e3
-    if world > 1:
-        t = torch.tensor([sec], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        sec = float(t.item())
+    sec = max_over_ranks(sec, world)
     updates_rank = n_model * STEPS_PER_BENCH_STEP * K
     events_rank = c1["events"] - c0["events"]
     spikes_rank = c1["spikes"] - c0["spikes"]
@@ -261,10 +276,7 @@ def run_ours(args):
         e2e_s += time.perf_counter() - t0
         h2d += int(m.sum()) * (8 + 4) + (STEPS_PER_BENCH_STEP + 1) * 8
         d2h += len(st) * 8 + 8
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, world)
 
     # roofline: algorithmic bytes of each kernel per launch (neuron state 32 B per
     # LIF/AdEx update, 48 B per HH update; 8 B per delivered event, +8 B when the
@@ -341,7 +353,7 @@ def run_sweep(args, rank, world):
     from edlut_b200.simulation import Simulation
     from edlut_b200.sweep import Sweep
     nsteps = args.sweep_steps
-    specs = sweep_networks(seed=1 + rank, n_networks=args.sweep_networks, t_end=nsteps * DT)
+    specs = sweep_networks(seed=rank_seed(1, rank), n_networks=args.sweep_networks, t_end=nsteps * DT)
     sw = Sweep.from_specs(specs, n_steps_max=nsteps)
     tune = sw.autotune(min(500, nsteps))
     stream = torch.cuda.ExternalStream(sw.stream())
@@ -356,10 +368,7 @@ def run_sweep(args, rank, world):
         sw.sync()
         times.append(a.elapsed_time(b) / 1e3)
     sec = statistics.mean(times)
-    if world > 1:
-        t = torch.tensor([sec], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        sec = float(t.item())
+    sec = max_over_ranks(sec, world)
     info = sw.info()
     sizes = np.array([sp["n"] for sp in specs])
     # plain path, one network at a time, on networks spread over the size range
@@ -411,7 +420,7 @@ def run_adjoint(args, rank, world):
     from edlut_b200.adjoint import TraceModel
     from edlut_b200.configs import adjoint_networks, perturbed_params
     B, n, steps, every = args.adjoint_networks, args.adjoint_neurons, args.adjoint_steps, 100
-    specs = adjoint_networks(seed=7 + rank, n_networks=B, n=n, t_end=steps * DT)
+    specs = adjoint_networks(seed=rank_seed(7, rank), n_networks=B, n=n, t_end=steps * DT)
     obs = np.stack([np.random.default_rng([7, i]).choice(n, 256, replace=False) for i in range(B)])
     model = TraceModel(specs, steps, obs, integrator="RK2", checkpoint_every=every)
     rng = np.random.default_rng(99)
@@ -447,8 +456,8 @@ def run_adjoint(args, rank, world):
         return min(out)
     fwd_only()
     fwd_bwd()
-    t_f = timed(fwd_only)
-    t_fb = timed(fwd_bwd)
+    t_f = max_over_ranks(timed(fwd_only), world)
+    t_fb = max_over_ranks(timed(fwd_bwd), world)
     loss = float(fwd_bwd().detach())
     gp = params.grad.numpy()
     gw = weights.grad
