@@ -154,13 +154,17 @@ def roofline_bytes(net, pop_events, pop_spikes, n_int):
             if frac_plastic > 0:
                 per_neuron = int((in_pop & plastic).sum()) / max(1, l.n)
                 out["post_stdp[%s]" % l.name] = EVENT_BYTES * per_neuron * pop_spikes[q] / n_int
+                # deferred form: one flush per 64 steps applies their post spikes
+                out["flush_post[%s]" % l.name] = 64 * out["post_stdp[%s]" % l.name]
         # fan-out launched from this population's spikes: 8 B per event it writes
         from_pop = (src >= starts[q]) & (src < starts[q + 1])
         if from_pop.any():
             tq = np.searchsorted(starts, tgt[from_pop], side="right") - 1
             ev_out = sum(pop_events[t] for t in set(tq.tolist()))
-            key = "input_push[-]" if l.model == "InputSpikeNeuronModel" else "push[%s]" % l.name
-            out[key] = EVENT_BYTES * ev_out / n_int
+            # input spikes fan out in their own kernel; model neurons' spikes inside the
+            # population's update kernel
+            key = "input_push[-]" if l.model == "InputSpikeNeuronModel" else "update[%s]" % l.name
+            out[key] = out.get(key, 0.0) + EVENT_BYTES * ev_out / n_int
     return out
 
 
@@ -247,7 +251,7 @@ def run_ours(args):
     tms = (ctypes.c_double * cap)()
     _lib.check(L.eb_get_profile(sim._h, cap, ctypes.byref(n), kinds, popi, lau, tms))
     _lib.check(L.eb_set_profile(sim._h, 0))
-    kind_names = {0: "input_push", 1: "update", 2: "post_stdp", 3: "push"}
+    kind_names = {0: "input_push", 1: "update", 2: "post_stdp", 3: "push", 4: "flush_post"}
     prof = []
     for i in range(n.value):
         pname = net.layers[popi[i]].name if popi[i] >= 0 else "-"
@@ -290,7 +294,8 @@ def run_ours(args):
         p["achieved_gbs"] = p["alg_bytes_per_launch"] / (p["avg_us"] * 1e-6) / 1e9
     top = prof[0]
     achieved = top["achieved_gbs"]
-    step_bytes = sum(alg.get(p["kernel"], 0.0) for p in prof)
+    n_prof_steps = prof_steps * STEPS_PER_BENCH_STEP
+    step_bytes = sum(alg.get(p["kernel"], 0.0) * p["launches"] for p in prof) / n_prof_steps
     step_gbs = step_bytes / (sec / n_int) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")

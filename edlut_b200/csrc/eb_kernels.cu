@@ -63,6 +63,35 @@ __device__ __forceinline__ void stdp_pre(const NetDev &N, uint32_t tp, const Syn
     s->last = a;
 }
 
+// STDPWeightChange::ApplyPostSynapticSpike on a synapse record for a spike of its
+// target at time t (src/learning_rules/STDPWeightChange.cpp:58-76).
+__device__ __forceinline__ void stdp_post(const NetDev &N, SynRec &r, double t) {
+    const float *rp = N.rule_par + r.rule * 6;
+    const float el = (float)(t - r.last);
+    float pre = r.pre * expt_net(N, -el * rp[4]);
+    float post = r.post * expt_net(N, -el * rp[5]);
+    post += 1.0f;
+    float w = r.w + rp[0] * pre;
+    if (w > r.maxw) w = r.maxw; else if (w < 0.0f) w = 0.0f;
+    r.w = w;
+    r.pre = pre;
+    r.post = post;
+    r.last = t;
+}
+
+// Deferred post-synaptic STDP: apply to record r of a plastic synapse onto
+// neuron i the target's spikes it has not seen (time > r.last), oldest first --
+// the same updates in the same order as at each spike, only later.  Every spike
+// of the ring is at most the arrival time being processed (spikes of this step
+// are recorded after the fold), and at an equal time the spike came first.
+__device__ __forceinline__ void apply_pending_post(const PopDev &P, const NetDev &N, int64_t i, SynRec &r) {
+    const uint32_t c = P.post_n[i];
+    const uint32_t lim = c < (uint32_t)kPostRing ? c : (uint32_t)kPostRing;
+    uint32_t np = 0;
+    while (np < lim && P.post_t[(int64_t)((c - 1 - np) % kPostRing) * P.n + i] > r.last) ++np;
+    for (uint32_t q = np; q > 0; --q) stdp_post(N, r, P.post_t[(int64_t)((c - q) % kPostRing) * P.n + i]);
+}
+
 template <int ND>
 __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
     if (ty == 0) x[ND] += w;
@@ -70,13 +99,22 @@ __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
     else x[ND + 2] += w;
 }
 
-// Apply one arrival: g[type] += w (weight before plasticity), then STDP pre.
+// Apply one arrival at neuron i: g[type] += w (weight before plasticity), then
+// STDP pre (after the target's deferred post updates, when it keeps a ring).
 template <int ND>
-__device__ __forceinline__ void apply_arrival(const NetDev &N, const Arrival &r, float *x) {
+__device__ __forceinline__ void apply_arrival(const PopDev &P, const NetDev &N, int64_t i, const Arrival &r, float *x) {
     const uint32_t tp = r.tpos;
-    const SynRec s = N.syn[tp];
+    SynRec s = N.syn[tp];
+    if (s.rule >= 0 && P.post_t) apply_pending_post(P, N, i, s);
     add_conductance<ND>(x, s.stype, s.w);
     if (s.rule >= 0) stdp_pre(N, tp, s, r.a);
+}
+
+// Record a spike of neuron i at step k for deferred post-synaptic STDP.
+__device__ __forceinline__ void note_post_spike(const PopDev &P, const NetDev &N, int64_t i, int64_t k) {
+    const uint32_t c = P.post_n[i];
+    P.post_t[(int64_t)(c % kPostRing) * P.n + i] = N.tstep[k];
+    P.post_n[i] = c + 1;
 }
 
 __device__ __forceinline__ int64_t cur_step(const NetDev &N, int rel) { return *N.step + rel + 1; }
@@ -158,6 +196,74 @@ __device__ __forceinline__ void compact_spikes(const PopDev &P, const NetDev &N,
     }
 }
 
+// ------------------------------------------------------------ spike fan-out --
+// Arrival step of a delivery at time a: the first update time strictly after a
+// (never below k_lo).  The guess floor(a/dt)+1 is confirmed by two independent
+// table reads in the common case; the loops only run when it is off by rounding.
+__device__ __forceinline__ int64_t arrival_step(const NetDev &N, double a, int64_t k_lo, double inv_dt) {
+    int64_t ka = (int64_t)(a * inv_dt) + 1;
+    if (ka < k_lo) ka = k_lo;
+    const double lo = N.tstep[ka - 1], hi = N.tstep[ka];
+    if (hi > a && (lo <= a || ka == k_lo)) return ka;
+    while (N.tstep[ka] <= a) ++ka;
+    while (ka > k_lo && N.tstep[ka - 1] > a) --ka;
+    return ka;
+}
+
+// Reserve a bucket entry of the target for step ka and store the arrival.
+// Loads that do not depend on the reservation are issued before the atomic.
+__device__ __forceinline__ void bucket_put(const NetDev &N, int64_t ka, double a, int64_t o) {
+    const uint32_t tg = N.out_tgt[o];
+    const uint32_t tp = N.out_tpos[o];
+    const uint32_t capg = N.cap[tg];
+    const int64_t base = N.cap_base[tg];
+    const int slot = (int)(ka % N.R);
+    const uint32_t idx = atomicAdd(N.cnt + (int64_t)slot * N.n_neurons + tg, 1u);
+    if (idx < capg) {
+        Arrival v;
+        v.a = a;
+        v.spos = (uint32_t)o;
+        v.tpos = tp;
+        N.rec[(int64_t)slot * N.cap_total + base + idx] = v;
+    } else {
+        atomicOr(N.flags, FLAG_BUCKET_OVERFLOW);
+    }
+}
+
+// One spike of population P at step k (update time t_k): the block's threads
+// cover the source's out-synapses (sorted by delay, then target).
+// Fan-out of source neuron src's spike at step k: lanes lane, lane + width, ...
+// of the caller's group take its out-synapses.
+__device__ __forceinline__ void push_from(const PopDev &P, const NetDev &N, int64_t k, int64_t src, int lane, int width,
+                                          double inv_dt) {
+    const double tk = P.kind == KIND_POISSON ? N.tgen[k] : N.tstep[k];  // generators spike on their own grid
+    const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
+    for (int64_t o = o0 + lane; o < o1; o += width) {
+        const double a = tk + (double)N.out_units[o] * 0.0001;
+        bucket_put(N, arrival_step(N, a, k + 1, inv_dt), a, o);
+    }
+}
+
+__device__ __forceinline__ void push_spike(const PopDev &P, const NetDev &N, int64_t k, int64_t s, double inv_dt) {
+    push_from(P, N, k, P.first + P.spk[s], threadIdx.x, blockDim.x, inv_dt);
+}
+
+// Fan-out inside the update kernel (graph path): a spike at step k only reaches
+// buckets of steps >= k+1, which no kernel of this step reads, so the spiking
+// warp delivers it at once instead of a separate launch after the update.  The
+// warp takes its spiking lanes one at a time, lanes over the out-synapses.
+__device__ __forceinline__ void warp_push(const PopDev &P, const NetDev &N, int64_t k, int64_t i, bool sp,
+                                          double inv_dt) {
+    unsigned m = __ballot_sync(0xffffffffu, sp);
+    const int lane = threadIdx.x & 31;
+    while (m) {
+        const int l = __ffs(m) - 1;
+        m &= m - 1u;
+        const int64_t src = P.first + __shfl_sync(0xffffffffu, i, l);
+        push_from(P, N, k, src, lane, 32, inv_dt);
+    }
+}
+
 // ----------------------------------------------------------- narrow update --
 // One thread per neuron.  Arrivals of this step are sorted in registers
 // (insertion sort; at most 16 in the fast path) and folded in order.
@@ -165,7 +271,8 @@ constexpr int kLocalSort = 16;
 constexpr int kNarrowTile = 256;
 
 template <int KIND, int INTEG>
-__device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev &N, int64_t k, int64_t tile) {
+__device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev &N, int64_t k, int64_t tile,
+                                                   double push_inv_dt = 0.0) {
     constexpr int ND = Model<KIND>::ND;
     const int64_t i = tile * kNarrowTile + threadIdx.x;
     const bool active = i < P.n;
@@ -184,7 +291,7 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
             if (c > capg) { atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
             Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
             if (c == 1) {
-                apply_arrival<ND>(N, r[0], x);
+                apply_arrival<ND>(P, N, i, r[0], x);
             } else if (c <= kLocalSort) {
                 Arrival loc[kLocalSort];
                 for (uint32_t a = 0; a < c; ++a) {
@@ -193,7 +300,7 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
                     while (b >= 0 && arr_less(v, loc[b])) { loc[b + 1] = loc[b]; --b; }
                     loc[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, loc[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, loc[a], x);
             } else {
                 for (uint32_t a = 1; a < c; ++a) {  // in-place insertion sort (rare path)
                     Arrival v = r[a];
@@ -201,12 +308,13 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
                     while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
                     r[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, r[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
             }
         }
         sp = advance_neuron<KIND, INTEG>(P, N, i, x);
         store_state<KIND>(P, i, x);
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
+        if (sp && P.post_t) note_post_spike(P, N, i, k);
     }
     // delivered-event counter: one atomic per warp
     unsigned long long cw = c;
@@ -214,13 +322,15 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
     for (int o = 16; o > 0; o >>= 1) cw += __shfl_down_sync(0xffffffffu, cw, o);
     if ((threadIdx.x & 31) == 0 && cw) atomicAdd(P.events, cw);
     compact_spikes(P, N, k, i, sp);
+    if (push_inv_dt > 0.0) warp_push(P, N, k, i, sp, push_inv_dt);
 }
 
+// push_inv_dt > 0: also fan out this step's spikes (1 / step, for arrival_step).
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kNarrowTile) k_update_narrow(PopDev P, NetDev N, int rel) {
+__global__ void __launch_bounds__(kNarrowTile) k_update_narrow(PopDev P, NetDev N, int rel, double push_inv_dt) {
     const int64_t k = cur_step(N, rel);
     if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
-    update_narrow_tile<KIND, INTEG>(P, N, k, blockIdx.x);
+    update_narrow_tile<KIND, INTEG>(P, N, k, blockIdx.x, push_inv_dt);
 }
 
 // ------------------------------------------------------------- wide update --
@@ -237,6 +347,7 @@ constexpr int kWideSmem = 1024;
 constexpr int kRankSort = 256;  // up to this many arrivals: rank sort (one pass), else bitonic
 
 struct WideSmem {
+    int spiked;  // the block's neuron spiked this step (fused fan-out)
     Arrival sbuf[kWideSmem];
     Arrival sorted[kRankSort];
     float sw[kWideSmem];
@@ -245,8 +356,10 @@ struct WideSmem {
 
 // STDP pre hook for one arrival with every synapse load issued up front (they
 // only depend on tp); returns the weight before the update through w_old.
-__device__ __forceinline__ void stdp_pre_gather(const NetDev &N, uint32_t tp, double a, float &w_old, int &ty) {
-    const SynRec r = N.syn[tp];
+__device__ __forceinline__ void stdp_pre_gather(const PopDev &P, const NetDev &N, int64_t i, uint32_t tp, double a,
+                                                float &w_old, int &ty) {
+    SynRec r = N.syn[tp];
+    if (r.rule >= 0 && P.post_t) apply_pending_post(P, N, i, r);
     w_old = r.w;
     ty = r.stype;
     if (r.rule < 0) return;
@@ -285,7 +398,8 @@ __device__ __forceinline__ void ordered_sum(float *x, const float *sw, const uin
 }
 
 template <int KIND, int INTEG>
-__device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S) {
+__device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
+                                                   double push_inv_dt = 0.0) {
     constexpr int ND = Model<KIND>::ND;
     const int tid = threadIdx.x;
     const int slot = (int)(k % N.R);
@@ -342,13 +456,13 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
             }
             if (P.may_repeat) {
                 if (tid == 0)
-                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, ord[a], x);
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, ord[a], x);
             } else {
                 for (int a = tid; a < (int)c; a += blockDim.x) {
                     const Arrival v = ord[a];
                     float w_old;
                     int ty;
-                    stdp_pre_gather(N, v.tpos, v.a, w_old, ty);
+                    stdp_pre_gather(P, N, i, v.tpos, v.a, w_old, ty);
                     S.sw[a] = w_old;
                     S.sty[a] = (uint8_t)ty;
                 }
@@ -362,12 +476,14 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
                 while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
                 r[b + 1] = v;
             }
-            for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(N, r[a], x);
+            for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
         }
         if (tid == 0) atomicAdd(P.events, (unsigned long long)c);
     }
     if (tid == 0) {
         const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x);
+        S.spiked = sp ? 1 : 0;
+        if (sp && P.post_t) note_post_spike(P, N, i, k);
         store_state<KIND>(P, i, x);
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
         if (sp) {
@@ -383,14 +499,15 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
         }
     }
     __syncthreads();
+    if (push_inv_dt > 0.0 && S.spiked) push_from(P, N, k, gi, tid, blockDim.x, push_inv_dt);
 }
 
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel) {
+__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel, double push_inv_dt) {
     __shared__ WideSmem S;
     const int64_t k = cur_step(N, rel);
     if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
-    for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) update_wide_neuron<KIND, INTEG>(P, N, k, i, S);
+    for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) update_wide_neuron<KIND, INTEG>(P, N, k, i, S, push_inv_dt);
 }
 
 // PoissonGeneratorDeviceVector::UpdateState (src/neuron_model/PoissonGeneratorDeviceVector.cpp:56-70):
@@ -399,7 +516,7 @@ __global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N
 // (include/simulation/RandomGenerator.h:91-107) -- and fires when
 // frequency * step > frand.  The low 31 bits of the product only depend on its low
 // 32 bits, so 32-bit arithmetic gives the reference's sequence.
-__global__ void __launch_bounds__(256) k_update_poisson(PopDev P, NetDev N, int rel) {
+__global__ void __launch_bounds__(256) k_update_poisson(PopDev P, NetDev N, int rel, double push_inv_dt) {
     const int64_t k = cur_step(N, rel);
     if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -414,54 +531,10 @@ __global__ void __launch_bounds__(256) k_update_poisson(PopDev P, NetDev N, int 
         }
     }
     compact_spikes(P, N, k, i, sp);
+    if (push_inv_dt > 0.0) warp_push(P, N, k, i, sp, push_inv_dt);
 }
 
 // ------------------------------------------------------------ spike fan-out --
-// Arrival step of a delivery at time a: the first update time strictly after a
-// (never below k_lo).  The guess floor(a/dt)+1 is confirmed by two independent
-// table reads in the common case; the loops only run when it is off by rounding.
-__device__ __forceinline__ int64_t arrival_step(const NetDev &N, double a, int64_t k_lo, double inv_dt) {
-    int64_t ka = (int64_t)(a * inv_dt) + 1;
-    if (ka < k_lo) ka = k_lo;
-    const double lo = N.tstep[ka - 1], hi = N.tstep[ka];
-    if (hi > a && (lo <= a || ka == k_lo)) return ka;
-    while (N.tstep[ka] <= a) ++ka;
-    while (ka > k_lo && N.tstep[ka - 1] > a) --ka;
-    return ka;
-}
-
-// Reserve a bucket entry of the target for step ka and store the arrival.
-// Loads that do not depend on the reservation are issued before the atomic.
-__device__ __forceinline__ void bucket_put(const NetDev &N, int64_t ka, double a, int64_t o) {
-    const uint32_t tg = N.out_tgt[o];
-    const uint32_t tp = N.out_tpos[o];
-    const uint32_t capg = N.cap[tg];
-    const int64_t base = N.cap_base[tg];
-    const int slot = (int)(ka % N.R);
-    const uint32_t idx = atomicAdd(N.cnt + (int64_t)slot * N.n_neurons + tg, 1u);
-    if (idx < capg) {
-        Arrival v;
-        v.a = a;
-        v.spos = (uint32_t)o;
-        v.tpos = tp;
-        N.rec[(int64_t)slot * N.cap_total + base + idx] = v;
-    } else {
-        atomicOr(N.flags, FLAG_BUCKET_OVERFLOW);
-    }
-}
-
-// One spike of population P at step k (update time t_k): the block's threads
-// cover the source's out-synapses (sorted by delay, then target).
-__device__ __forceinline__ void push_spike(const PopDev &P, const NetDev &N, int64_t k, int64_t s, double inv_dt) {
-    const double tk = P.kind == KIND_POISSON ? N.tgen[k] : N.tstep[k];  // generators spike on their own grid
-    const int64_t src = P.first + P.spk[s];
-    const int64_t o0 = N.out_ptr[src], o1 = N.out_ptr[src + 1];
-    for (int64_t o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-        const double a = tk + (double)N.out_units[o] * 0.0001;
-        bucket_put(N, arrival_step(N, a, k + 1, inv_dt), a, o);
-    }
-}
-
 // One input-neuron spike q emitted in [t_{k-1}, t_k).  A source with several
 // distinct delays delivers group j+1 at (a_j - d_j) + d_{j+1}, as the reference's
 // PropagatedSpike chain does.
@@ -779,33 +852,33 @@ __global__ void k_advance(int64_t *step, int K) { *step += K; }
 
 // ------------------------------------------------------------------ launch --
 template <int KIND, int INTEG>
-static void launch_update_t(const PopDev &P, const NetDev &N, int rel, cudaStream_t st) {
+static void launch_update_t(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st) {
     if (P.wide) {
         const int blocks = (int)std::min<int64_t>(P.n, 148 * 8);
-        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, 0, st>>>(P, N, rel);
+        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, 0, st>>>(P, N, rel, push_inv_dt);
     } else {
         const int blocks = (int)((P.n + 255) / 256);
-        k_update_narrow<KIND, INTEG><<<blocks, 256, 0, st>>>(P, N, rel);
+        k_update_narrow<KIND, INTEG><<<blocks, 256, 0, st>>>(P, N, rel, push_inv_dt);
     }
 }
 
 template <int KIND>
-static void launch_update_k(const PopDev &P, const NetDev &N, int rel, cudaStream_t st) {
+static void launch_update_k(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st) {
     switch (P.integ) {
-    case INTEG_EULER: launch_update_t<KIND, INTEG_EULER>(P, N, rel, st); break;
-    case INTEG_RK2: launch_update_t<KIND, INTEG_RK2>(P, N, rel, st); break;
-    case INTEG_RK4: launch_update_t<KIND, INTEG_RK4>(P, N, rel, st); break;
-    default: launch_update_t<KIND, INTEG_BDF>(P, N, rel, st); break;
+    case INTEG_EULER: launch_update_t<KIND, INTEG_EULER>(P, N, rel, push_inv_dt, st); break;
+    case INTEG_RK2: launch_update_t<KIND, INTEG_RK2>(P, N, rel, push_inv_dt, st); break;
+    case INTEG_RK4: launch_update_t<KIND, INTEG_RK4>(P, N, rel, push_inv_dt, st); break;
+    default: launch_update_t<KIND, INTEG_BDF>(P, N, rel, push_inv_dt, st); break;
     }
 }
 
-void launch_update(const PopDev &P, const NetDev &N, int rel, cudaStream_t st) {
+void launch_update(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st) {
     if (P.n <= 0) return;
     switch (P.kind) {
-    case KIND_LIF: launch_update_k<KIND_LIF>(P, N, rel, st); break;
-    case KIND_ADEX: launch_update_k<KIND_ADEX>(P, N, rel, st); break;
-    case KIND_HH: launch_update_k<KIND_HH>(P, N, rel, st); break;
-    case KIND_POISSON: k_update_poisson<<<(unsigned)((P.n + 255) / 256), 256, 0, st>>>(P, N, rel); break;
+    case KIND_LIF: launch_update_k<KIND_LIF>(P, N, rel, push_inv_dt, st); break;
+    case KIND_ADEX: launch_update_k<KIND_ADEX>(P, N, rel, push_inv_dt, st); break;
+    case KIND_HH: launch_update_k<KIND_HH>(P, N, rel, push_inv_dt, st); break;
+    case KIND_POISSON: k_update_poisson<<<(unsigned)((P.n + 255) / 256), 256, 0, st>>>(P, N, rel, push_inv_dt); break;
     default: break;
     }
 }
@@ -820,6 +893,37 @@ void launch_input_push(const NetDev &N, int rel, double inv_dt, int blocks, int 
 
 void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks, int blocks, cudaStream_t st) {
     k_post_stdp<<<blocks, kPostThreads, 0, st>>>(P, N, rel, max_chunks);
+}
+
+// Bring every plastic synapse onto the population up to date with its target's
+// deferred post-synaptic spikes: items are (neuron, chunk of kPostThreads plastic
+// synapses), neurons without spikes since the last flush skipped.
+__global__ void __launch_bounds__(kPostThreads) k_flush_post(PopDev P, NetDev N, int max_chunks) {
+    const int64_t items = P.n * (int64_t)max_chunks;
+    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const int64_t i = item / max_chunks, ch = item % max_chunks;
+        if (P.post_n[i] == P.post_flushed[i]) continue;
+        const int64_t t = P.first + i;
+        const int64_t tp = N.in_ptr[t] + ch * kPostThreads + threadIdx.x;
+        if (tp >= N.plastic_end[t]) continue;
+        SynRec r = N.syn[tp];
+        apply_pending_post(P, N, i, r);
+        SynRec *o = N.syn + tp;
+        o->w = r.w;
+        o->pre = r.pre;
+        o->post = r.post;
+        o->last = r.last;
+    }
+}
+
+__global__ void k_flush_mark(PopDev P) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x)
+        P.post_flushed[i] = P.post_n[i];
+}
+
+void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, int blocks, cudaStream_t st) {
+    k_flush_post<<<blocks, kPostThreads, 0, st>>>(P, N, max_chunks);
+    k_flush_mark<<<(unsigned)std::min<int64_t>((P.n + 255) / 256, 1184), 256, 0, st>>>(P);
 }
 
 void launch_advance(int64_t *step, int K, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(step, K); }

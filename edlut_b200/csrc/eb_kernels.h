@@ -4,11 +4,14 @@
 #include "eb_types.h"
 
 namespace eb {
-void launch_update(const PopDev &P, const NetDev &N, int rel, cudaStream_t st);
+// push_inv_dt > 0: the update kernel also fans out the step's spikes (no launch_push).
+void launch_update(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st);
 constexpr int kPostThreads = 256;  // plastic synapses per post-STDP work item
 void launch_push(const PopDev &P, const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st);
 void launch_input_push(const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st);
 void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks, int blocks, cudaStream_t st);
+// Deferred post-synaptic STDP: apply the spikes noted since the last flush (2 launches).
+void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, int blocks, cudaStream_t st);
 void launch_advance(int64_t *step, int K, cudaStream_t st);
 
 constexpr int kMaxPersistPops = 16;

@@ -432,6 +432,16 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         D.wide = maxcap > 16 ? 1 : 0;
         p.has_plastic_in = max_plastic > 0;
         p.post_chunks = (int)((max_plastic + kPostThreads - 1) / kPostThreads);
+        if (p.has_plastic_in) {
+            // deferred post-synaptic STDP (graph path): a ring of recent spike times
+            lazy_post = true;
+            if ((rc = dalloc((void **)&D.post_t, sizeof(double) * (size_t)kPostRing * p.n))) return rc;
+            if ((rc = dalloc((void **)&D.post_n, sizeof(uint32_t) * (size_t)p.n))) return rc;
+            if ((rc = dalloc((void **)&D.post_flushed, sizeof(uint32_t) * (size_t)p.n))) return rc;
+            CK(cudaMemsetAsync(D.post_t, 0, sizeof(double) * (size_t)kPostRing * p.n, st));
+            CK(cudaMemsetAsync(D.post_n, 0, sizeof(uint32_t) * (size_t)p.n, st));
+            CK(cudaMemsetAsync(D.post_flushed, 0, sizeof(uint32_t) * (size_t)p.n, st));
+        }
         p.has_out = false;
         int64_t max_out = 0, in_from_inputs = 0;
         for (int64_t i = p.first; i < p.first + p.n; ++i) {
@@ -463,6 +473,11 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         }
         dyn.push_back({p.dev.spk_count, 2 * sizeof(uint32_t)});
         if (p.dev.lcg) dyn.push_back({p.dev.lcg, sizeof(uint32_t) * (size_t)p.n});
+        if (p.dev.post_t) {
+            dyn.push_back({p.dev.post_t, sizeof(double) * (size_t)kPostRing * p.n});
+            dyn.push_back({p.dev.post_n, sizeof(uint32_t) * (size_t)p.n});
+            dyn.push_back({p.dev.post_flushed, sizeof(uint32_t) * (size_t)p.n});
+        }
     }
     for (int q = 0; q < 4; ++q) {
         cudaStream_t ss;
@@ -653,6 +668,29 @@ void eb_ctx::fork_join(std::vector<std::function<void(cudaStream_t)>> &work) {
     }
 }
 
+// Deferred post-synaptic STDP: apply every noted spike to the synapses (on the
+// context stream, profiled as kind 4).  Runs at least every kPostRing steps.
+void eb_ctx::enqueue_flush() {
+    steps_since_flush = 0;
+    for (size_t q = 0; q < pops.size(); ++q) {
+        const auto &p = pops[q];
+        if (!p.dev.post_t) continue;
+        cudaEvent_t a = nullptr;
+        prof_stream = stream;
+        prof_begin(4, (int)q, &a);
+        enq_count += 2;
+        launch_flush_post(p.dev, net, std::max(1, p.post_chunks), 148 * 4, stream);
+        prof_end(4, (int)q, a);
+    }
+}
+
+int eb_ctx::flush_post() {
+    if (!lazy_post || !finalized) return EB_OK;
+    enqueue_flush();
+    CK(cudaGetLastError());
+    return EB_OK;
+}
+
 void eb_ctx::enqueue_step(int rel) {
     const int fan_blocks = 148 * 4;
     const double inv_dt = 1.0 / dt_s;
@@ -676,21 +714,22 @@ void eb_ctx::enqueue_step(int rel) {
     }
     for (size_t q = 0; q < pops.size(); ++q) {
         if (pops[q].kind == KIND_INPUT) continue;
-        phase.push_back(timed(1, (int)q, [this, q, rel](cudaStream_t s) { launch_update(pops[q].dev, net, rel, s); }));
+        // spikes fan out inside the update kernel (arrivals land at step k+1 or later)
+        const double push_inv_dt = pops[q].has_out ? inv_dt : 0.0;
+        phase.push_back(timed(1, (int)q, [this, q, rel, push_inv_dt](cudaStream_t s) {
+            launch_update(pops[q].dev, net, rel, push_inv_dt, s);
+        }));
     }
     fork_join(phase);
     phase.clear();
     for (size_t q = 0; q < pops.size(); ++q) {
         auto &p = pops[q];
         if (p.kind == KIND_INPUT) continue;
-        if (p.has_plastic_in)
+        if (p.has_plastic_in && !p.dev.post_t)
             phase.push_back(timed(2, (int)q, [this, q, rel, fan_blocks](cudaStream_t s) {
                 launch_post_stdp(pops[q].dev, net, rel, pops[q].post_chunks, fan_blocks, s);
             }));
-        if (p.has_out)
-            phase.push_back(timed(3, (int)q, [this, q, rel, inv_dt, fan_blocks](cudaStream_t s) {
-                launch_push(pops[q].dev, net, rel, inv_dt, fan_blocks, pops[q].push_threads, s);
-            }));
+
     }
     fork_join(phase);
 }
@@ -754,6 +793,7 @@ int eb_ctx::build_graph(int K) {
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     enq_count = 0;
     for (int r = 0; r < K; ++r) enqueue_step(r);
+    if (lazy_post) enqueue_flush();
     graph_kernels = enq_count + 1;
     launch_advance(d_step, K, stream);
     CK(cudaStreamEndCapture(stream, &g));
@@ -778,12 +818,20 @@ int eb_ctx::run_async(int64_t n) {
         graphs_valid = false;
     }
     int K = graph_steps > 0 ? graph_steps : 64;
+    if (lazy_post && K > kPostRing) K = kPostRing;  // a graph's spikes must fit the rings
     int64_t done = 0;
     if (persistent && persist_ok && !profile) {
         if (pops_dirty) {
+            // the persistent kernel applies post-synaptic STDP at each spike (its own
+            // phase); every run ends with a flush, so no deferred spike is pending here
             std::vector<PopDev> h;
             for (auto &p : pops)
-                if (p.kind != KIND_INPUT) h.push_back(p.dev);
+                if (p.kind != KIND_INPUT) {
+                    h.push_back(p.dev);
+                    h.back().post_t = nullptr;
+                    h.back().post_n = nullptr;
+                    h.back().post_flushed = nullptr;
+                }
             CK(cudaMemcpyAsync(d_pops, h.data(), sizeof(PopDev) * h.size(), cudaMemcpyHostToDevice, stream));
             pops_dirty = false;
         }
@@ -805,7 +853,11 @@ int eb_ctx::run_async(int64_t n) {
         cudaGraphExec_t ge;
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         enq_count = 0;
-        for (int64_t r = 0; r < n; ++r) enqueue_step((int)r);
+        for (int64_t r = 0; r < n; ++r) {
+            enqueue_step((int)r);
+            if (lazy_post && (r + 1) % kPostRing == 0) enqueue_flush();
+        }
+        if (lazy_post) enqueue_flush();
         launch_advance(d_step, (int)n, stream);
         CK(cudaStreamEndCapture(stream, &g));
         CK(cudaGraphInstantiate(&ge, g, 0));
@@ -830,8 +882,14 @@ int eb_ctx::run_async(int64_t n) {
         enq_count = 0;
         enqueue_step(0);
         launch_advance(d_step, 1, stream);
+        if (lazy_post && ++steps_since_flush == kPostRing) enqueue_flush();
         launches += enq_count + 1;
         done++;
+    }
+    if (lazy_post && steps_since_flush) {
+        enq_count = 0;
+        enqueue_flush();
+        launches += enq_count;
     }
     CK(cudaGetLastError());
     steps_done = k_end;

@@ -134,6 +134,10 @@ struct eb_ctx {
     int build_graph(int K);
     int setup_persistent();
     int seed_generators();
+    void enqueue_flush();
+    int flush_post();
+    bool lazy_post = false;       // some population defers post-synaptic STDP
+    int steps_since_flush = 0;
     int run_async(int64_t n);
     int sync();
     int snapshot(int slot);

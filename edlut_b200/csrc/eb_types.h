@@ -8,6 +8,7 @@ enum Kind : int { KIND_INPUT = 0, KIND_LIF = 1, KIND_ADEX = 2, KIND_HH = 3, KIND
 enum Integ : int { INTEG_EULER = 0, INTEG_RK2 = 1, INTEG_RK4 = 2, INTEG_BDF = 3 };
 
 constexpr int kMaxVars = 8;
+constexpr int kPostRing = 64;  // spikes kept per neuron for deferred post-synaptic STDP
 constexpr int kNmdaTable = 256;
 constexpr int kExptTable = 1024 * 16;
 constexpr int kHHTable = 1024 * 256;
@@ -74,6 +75,12 @@ struct PopDev {
     // Poisson generators: LCG state and firing threshold rate * step per neuron
     uint32_t *lcg;
     const double *pthr;
+    // Deferred post-synaptic STDP: the times of each neuron's recent spikes,
+    // post_t[slot * n + i] with slot = spike number % kPostRing, and spike counts;
+    // null when the population applies post-synaptic STDP eagerly.
+    double *post_t;
+    uint32_t *post_n;
+    uint32_t *post_flushed;  // post_n at the last flush
 };
 
 // Network-wide device pointers, passed by value to the kernels.
