@@ -216,6 +216,63 @@ def parity_network(model: str = "LIFTimeDrivenModel", integrator: str = "Euler",
     return net, times, cells + inp.start
 
 
+def wide_fanin_network(seed: int = 1, n_relay: int = 3000, n_target: int = 4, n_repeat: int = 2,
+                       n_direct: int = 40, bursts=(60, 200, 400, 512, 520, 800, 2000, 3000),
+                       gap_steps: int = 40, dt: float = 1e-4):
+    """Arrival-count coverage network for the block-per-neuron update: ``n_relay``
+    LIF relays, each driven by its own input, fire in bursts of the given sizes (half
+    of a burst one step after the other half), and project with delays 0.9 or 1.0 ms
+    onto ``n_target`` LIF targets (RK4, STDP) and ``n_repeat`` LIF targets (Euler,
+    STDP) that also receive ``n_direct`` inputs, some of which fire twice within one
+    step.  A burst of B relays delivers about B/2 arrivals in one step (the two
+    halves meet) and B/4 in the steps either side, so the defaults reach every
+    arrival-count regime of the update (tens, up to 256, up to 1024, beyond).
+    Returns (NetworkDescription, input_times, input_cells)."""
+    rng = np.random.default_rng(seed)
+    net = NetworkDescription()
+    inp = net.add_layer(Layer(n_relay + n_direct, "InputSpikeNeuronModel", output=0))
+    rel = net.add_layer(Layer(n_relay, "LIFTimeDrivenModel", dict(LIF_C1), integrator="RK2", dt=dt, name="relay"))
+    tgt = net.add_layer(Layer(n_target, "LIFTimeDrivenModel", dict(LIF_C1), integrator="RK4", dt=dt, name="target"))
+    rep = net.add_layer(Layer(n_repeat, "LIFTimeDrivenModel", dict(LIF_C1), integrator="Euler", dt=dt,
+                              name="repeat"))
+    w_max = 0.2
+    net.rules.append(("STDP", [0.05 * w_max, 0.020, 0.0525 * w_max, 0.020]))
+    # input j -> relay j: one spike of the relay per input spike
+    net.add_synapses(np.arange(n_relay) + inp.start, np.arange(n_relay) + rel.start, 1e-4, 0, 8.0, 8.0, -1)
+    for layer in (tgt, rep):
+        s = np.repeat(np.arange(n_relay), len(layer))
+        t = np.tile(np.arange(len(layer)), n_relay)
+        d = np.where(rng.random(len(s)) < 0.5, 0.9e-3, 1.0e-3).astype(np.float32)
+        w = (rng.random(len(s)) * w_max).astype(np.float32)
+        net.add_synapses(s + rel.start, t + layer.start, d, 0, w, np.float32(1.25 * w_max), 0)
+    s = np.repeat(np.arange(n_direct), n_repeat)
+    t = np.tile(np.arange(n_repeat), n_direct)
+    net.add_synapses(s + n_relay + inp.start, t + rep.start, 1e-3, 0,
+                     (rng.random(len(s)) * w_max).astype(np.float32), np.float32(1.25 * w_max), 0)
+    times, cells = [], []
+    for b, size in enumerate(bursts):
+        step = 20 + gap_steps * b
+        who = rng.choice(n_relay, size=min(size, n_relay), replace=False)
+        half = len(who) // 2
+        times.append(np.full(half, (step + 0.5) * dt))
+        times.append(np.full(len(who) - half, (step + 1.5) * dt))
+        cells.append(who)
+    t_end = (20 + gap_steps * len(bursts)) * dt
+    dt_in, dc_in = poisson_input_times(rng, n_direct, 200.0, t_end, dt)
+    times.append(dt_in)
+    cells.append(dc_in + n_relay)
+    # doublets: a direct input firing twice inside one step
+    for _ in range(12):
+        j = int(rng.integers(0, n_direct))
+        k = int(rng.integers(10, int(t_end / dt) - 10))
+        times.append(np.array([(k + 0.2) * dt, (k + 0.7) * dt]))
+        cells.append(np.array([j + n_relay, j + n_relay]))
+    times = np.concatenate(times)
+    cells = np.concatenate(cells).astype(np.int64)
+    o = np.lexsort((cells, times))
+    return net, times[o], cells[o] + inp.start
+
+
 # Parameters the adjoint differentiates, in the order of its gradient rows.
 ADJOINT_PARAMS = ("g_leak", "e_leak", "tau_exc", "tau_inh")
 

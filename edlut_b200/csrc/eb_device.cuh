@@ -37,26 +37,42 @@ __device__ __forceinline__ float nmda_inf(const PopDev &P, float v, float e_inh)
 }
 
 // -------------------------------------------------------------------- LIF --
-// x = {V, gE, gI, gNMDA}; refr = updates since the last spike (-1: never spiked,
-// LastSpikeTime >= 100 s).  LastSpikeTime = refr * dt exactly, because every
-// partial sum of the reference's double accumulation is exact.
-__device__ __forceinline__ void lif_deriv(const PopDev &P, const float *x, float *dx, int refr) {
+// Refractory state of one update: the reference's derivative decides from
+// l = LastSpikeTime (ms) against tau_ref on every call; the decision only depends
+// on the update count since the last spike, so it is taken once per update with
+// the same double arithmetic and the derivative calls apply it.
+struct Refr {
+    int mode;    // 0: free (full derivative), 1: partial (fraction * full), 2: refractory (0)
+    float frac;  // fraction of mode 1
+};
+
+// refr = updates since the last spike (-1: never spiked, LastSpikeTime >= 100 s).
+// LastSpikeTime = refr * dt exactly, because every partial sum of the reference's
+// double accumulation is exact.
+__device__ __forceinline__ Refr lif_refr(const PopDev &P, int refr) {
+    Refr r{0, 1.0f};
+    if (refr < 0) return r;
+    const double tref = (double)P.p[7];
+    const double l = ((double)refr * (double)P.dt_s) * 1000.0;
+    if (l > tref) return r;
+    if (l + (double)P.dt_ms > tref) {
+        r.mode = 1;
+        r.frac = (float)((l + (double)P.dt_ms - tref) / (double)P.dt_ms);
+    } else {
+        r.mode = 2;
+    }
+    return r;
+}
+
+// x = {V, gE, gI, gNMDA}
+__device__ __forceinline__ void lif_deriv(const PopDev &P, const float *x, float *dx, Refr rf) {
     const float *p = P.p;  // e_exc e_inh e_leak v_thr c_m tau_exc tau_inh tau_ref g_leak tau_nmda
     float current = 0.0f;
     if (P.en & 1) current += x[1] * (p[0] - x[0]);
     if (P.en & 2) current += x[2] * (p[1] - x[0]);
     if (P.en & 4) current += x[3] * nmda_inf(P, x[0], p[1]) * (p[0] - x[0]);
-    float full = (current + p[8] * (p[2] - x[0])) * P.inv_c_m;
-    if (refr < 0) { dx[0] = full; return; }
-    double l = ((double)refr * (double)P.dt_s) * 1000.0;
-    if (l > (double)p[7]) {
-        dx[0] = full;
-    } else if (l + (double)P.dt_ms > (double)p[7]) {
-        float fraction = (float)((l + (double)P.dt_ms - (double)p[7]) / (double)P.dt_ms);
-        dx[0] = fraction * full;
-    } else {
-        dx[0] = 0.0f;
-    }
+    const float full = (current + p[8] * (p[2] - x[0])) * P.inv_c_m;
+    dx[0] = rf.mode == 0 ? full : rf.mode == 1 ? rf.frac * full : 0.0f;
 }
 
 // ------------------------------------------------------------------- AdEx --
@@ -119,15 +135,15 @@ __device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
 template <int KIND> struct Model;
 template <> struct Model<KIND_LIF> {
     static constexpr int ND = 1, NV = 4;
-    __device__ static void deriv(const PopDev &P, float *x, float *dx, int refr) { lif_deriv(P, x, dx, refr); }
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr rf) { lif_deriv(P, x, dx, rf); }
 };
 template <> struct Model<KIND_ADEX> {
     static constexpr int ND = 2, NV = 5;
-    __device__ static void deriv(const PopDev &P, float *x, float *dx, int) { adex_deriv(P, x, dx); }
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr) { adex_deriv(P, x, dx); }
 };
 template <> struct Model<KIND_HH> {
     static constexpr int ND = 4, NV = 7;
-    __device__ static void deriv(const PopDev &P, float *x, float *dx, int) { hh_deriv(P, x, dx); }
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr) { hh_deriv(P, x, dx); }
 };
 
 // EvaluateTimeDependentEquation: g <- 0 below 1e-9, else g * factor (enabled types only).
@@ -211,36 +227,37 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
     constexpr int ND = M::ND, NV = M::NV;
     const float dt = P.dt_ms;
     float k1[NV], k2[NV], k3[NV], k4[NV], aux[NV];
+    const Refr rf = (KIND == KIND_LIF) ? lif_refr(P, refr) : Refr{0, 1.0f};
     if (INTEG == INTEG_EULER) {
-        M::deriv(P, x, k1, refr);
+        M::deriv(P, x, k1, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += dt * k1[j];
         decay<ND>(P, x);
     } else if (INTEG == INTEG_RK2) {
-        M::deriv(P, x, k1, refr);
+        M::deriv(P, x, k1, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += k1[j] * dt;
         decay<ND>(P, x);
-        M::deriv(P, x, k2, refr);
+        M::deriv(P, x, k2, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += (-k1[j] + k2[j]) * dt * 0.5f;
     } else if (INTEG == INTEG_RK4) {
         const float h05 = dt * 0.5f;
         const float h016 = dt * 0.166666666667f;
-        M::deriv(P, x, k1, refr);
+        M::deriv(P, x, k1, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) aux[j] = x[j] + k1[j] * h05;
 #pragma unroll
         for (int j = ND; j < NV; ++j) aux[j] = x[j];
         decay<ND>(P, aux);
-        M::deriv(P, aux, k2, refr);
+        M::deriv(P, aux, k2, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) aux[j] = x[j] + k2[j] * h05;
-        M::deriv(P, aux, k3, refr);
+        M::deriv(P, aux, k3, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) aux[j] = x[j] + k3[j] * dt;
         decay<ND>(P, aux);
-        M::deriv(P, aux, k4, refr);
+        M::deriv(P, aux, k4, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += (k1[j] + 2.0f * (k2[j] + k3[j]) + k4[j]) * h016;
 #pragma unroll
@@ -249,7 +266,7 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
         int st = bdf_state;
         float pr[NV], p1[ND], c[ND], jac[ND * ND], J[ND * ND], iJ[ND * ND];
         if (st == 0) {
-            M::deriv(P, x, aux, refr);
+            M::deriv(P, x, aux, rf);
 #pragma unroll
             for (int j = 0; j < ND; ++j) pr[j] = x[j] + dt * aux[j];
         } else {
@@ -272,7 +289,7 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
         const float eps_j = dt * 0.1f;
         const float inv_eps = 1.0f / eps_j;
         while (epsi > 1e-6 && k < 10) {
-            M::deriv(P, pr, aux, refr);
+            M::deriv(P, pr, aux, rf);
 #pragma unroll
             for (int j = 0; j < ND; ++j) {
                 c[j] = co[0] * dt * aux[j] + co[1] * x[j];
@@ -283,13 +300,13 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
                 float tmp[NV], pos[NV], neg[NV];
 #pragma unroll
                 for (int v = 0; v < NV; ++v) tmp[v] = pr[v];
-                M::deriv(P, tmp, pos, refr);
+                M::deriv(P, tmp, pos, rf);
 #pragma unroll
                 for (int j = 0; j < ND; ++j) {
 #pragma unroll
                     for (int v = 0; v < NV; ++v) tmp[v] = pr[v];
                     tmp[j] -= eps_j;
-                    M::deriv(P, tmp, neg, refr);
+                    M::deriv(P, tmp, neg, rf);
 #pragma unroll
                     for (int z = 0; z < ND; ++z) jac[z * ND + j] = (pos[z] - neg[z]) * inv_eps;
                 }

@@ -84,13 +84,31 @@ __device__ __forceinline__ void stdp_post(const NetDev &N, SynRec &r, double t) 
 // the same updates in the same order as at each spike, only later.  Every spike
 // of the ring is at most the arrival time being processed (spikes of this step
 // are recorded after the fold), and at an equal time the spike came first.
-__device__ __forceinline__ void apply_pending_post(const PopDev &P, const NetDev &N, int64_t i, SynRec &r) {
-    const uint32_t c = P.post_n[i];
+// The ring holds the target's last kPostRing spike times, slot = count % kPostRing,
+// in global memory (RingGlobal) or staged in shared memory (RingSmem).
+struct RingGlobal {
+    const double *t;
+    int64_t n, i;
+    __device__ double operator()(uint32_t slot) const { return t[(int64_t)slot * n + i]; }
+};
+struct RingSmem {
+    const double *t;
+    __device__ double operator()(uint32_t slot) const { return t[slot]; }
+};
+
+template <class Ring>
+__device__ __forceinline__ void apply_pending(const NetDev &N, Ring ring, uint32_t c, SynRec &r) {
     const uint32_t lim = c < (uint32_t)kPostRing ? c : (uint32_t)kPostRing;
     uint32_t np = 0;
-    while (np < lim && P.post_t[(int64_t)((c - 1 - np) % kPostRing) * P.n + i] > r.last) ++np;
-    for (uint32_t q = np; q > 0; --q) stdp_post(N, r, P.post_t[(int64_t)((c - q) % kPostRing) * P.n + i]);
+    while (np < lim && ring((c - 1 - np) % kPostRing) > r.last) ++np;
+    for (uint32_t q = np; q > 0; --q) stdp_post(N, r, ring((c - q) % kPostRing));
 }
+
+__device__ __forceinline__ void apply_pending_post(const PopDev &P, const NetDev &N, int64_t i, SynRec &r) {
+    apply_pending(N, RingGlobal{P.post_t, P.n, i}, P.post_n[i], r);
+}
+
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
 template <int ND>
 __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
@@ -133,12 +151,27 @@ __device__ __forceinline__ void store_state(const PopDev &P, int64_t i, const fl
     for (int v = 0; v < NV; ++v) if (P.x[v]) P.x[v][i] = x[v];
 }
 
+// Per-neuron integer state next to the variables: LIF updates since the last
+// spike, BDF history depth.
+struct NeuronAux {
+    int refr;
+    int bst;
+};
+
+template <int KIND, int INTEG>
+__device__ __forceinline__ NeuronAux load_aux(const PopDev &P, int64_t i) {
+    NeuronAux a;
+    a.refr = (KIND == KIND_LIF) ? P.refr[i] : -1;
+    a.bst = (INTEG == INTEG_BDF) ? (int)P.bdf_state[i] : 0;
+    return a;
+}
+
 // Advance one neuron (after its arrivals were folded); returns spike flag.
 template <int KIND, int INTEG>
-__device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N, int64_t i, float *x) {
+__device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N, int64_t i, float *x, NeuronAux ax) {
     constexpr int NV = Model<KIND>::NV;
-    int refr = (KIND == KIND_LIF) ? P.refr[i] : -1;
-    int bst = (INTEG == INTEG_BDF) ? (int)P.bdf_state[i] : 0;
+    int refr = ax.refr;
+    int bst = ax.bst;
     BdfRef H{P.bdf_D, P.bdf_P, P.n, i};
     const float prevV = x[0];
     if (!integrate<KIND, INTEG>(P, x, refr, bst, H)) atomicOr(N.flags, FLAG_BDF_SINGULAR);
@@ -156,6 +189,11 @@ __device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N,
     if (KIND == KIND_LIF) P.refr[i] = refr;
     if (INTEG == INTEG_BDF) P.bdf_state[i] = (int8_t)bst;
     return sp;
+}
+
+template <int KIND, int INTEG>
+__device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N, int64_t i, float *x) {
+    return advance_neuron<KIND, INTEG>(P, N, i, x, load_aux<KIND, INTEG>(P, i));
 }
 
 __device__ __forceinline__ void record_trace(const PopDev &P, const NetDev &N, int64_t k, int64_t gi, const float *x, int nv) {
@@ -335,24 +373,41 @@ __global__ void __launch_bounds__(kNarrowTile) k_update_narrow(PopDev P, NetDev 
 
 // ------------------------------------------------------------- wide update --
 // One block per neuron, for populations whose neurons receive many arrivals per
-// step (e.g. Purkinje-like cells with 10^4-10^5 inputs).  The block sorts the
-// arrivals in shared memory (bitonic, up to kWideSmem records), every thread
-// fetches the weight of one arrival and applies its STDP pre-synaptic update in
-// parallel (synapses are independent; a synapse that can arrive twice in one step
-// -- only from input neurons -- forces the serial path), and thread 0 adds the
-// weights into the conductances in delivery order, then integrates the neuron.
+// step (e.g. Purkinje-like cells with 10^4-10^5 inputs).
+//
+// Up to kRankSort arrivals, every arrival finds its delivery position by counting
+// the arrivals ordered before it -- (time, synapse order) compared as integers,
+// since the bits of a non-negative double order like its value -- with all the
+// block's threads sharing the comparisons.  Each arrival's synapse record is
+// fetched while the positions are counted, its STDP pre-synaptic update applied
+// in parallel (synapses are independent; a synapse that can arrive twice in one
+// step -- only from input neurons -- forces the serial path) and its weight stored
+// at its position; one thread per conductance then adds the weights in delivery
+// order.  Up to kWideSmem arrivals: bitonic sort in shared memory; beyond, a
+// serial insertion sort in global memory.
 constexpr int kWideThreads = 256;
 constexpr int kWideSmem = 1024;
-
-constexpr int kRankSort = 256;  // up to this many arrivals: rank sort (one pass), else bitonic
+constexpr int kRankSort = 256;
+static_assert(kRankSort <= kWideThreads && kWideThreads == kNarrowTile, "wide blocks rank with one thread per arrival");
 
 struct WideSmem {
-    int spiked;  // the block's neuron spiked this step (fused fan-out)
+    int spiked;                         // the block's neuron spiked this step (fused fan-out)
+    uint32_t ring_n;                    // post-synaptic spikes noted so far (deferred STDP)
+    float g[3];                         // conductances handed to the per-type adders
+    unsigned long long khi[kRankSort];  // arrival time keys
+    uint32_t klo[kRankSort];            // synapse order
+    uint32_t rank[kRankSort];           // delivery position
+    double ring[kPostRing];             // the neuron's deferred post-synaptic spike times
     Arrival sbuf[kWideSmem];
-    Arrival sorted[kRankSort];
     float sw[kWideSmem];
     uint8_t sty[kWideSmem];
 };
+
+// Order-preserving integer key of an arrival time (-0 folded into +0).
+__device__ __forceinline__ unsigned long long time_key(double a) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(a + 0.0);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
 
 // STDP pre hook for one arrival with every synapse load issued up front (they
 // only depend on tp); returns the weight before the update through w_old.
@@ -366,100 +421,142 @@ __device__ __forceinline__ void stdp_pre_gather(const PopDev &P, const NetDev &N
     stdp_pre(N, tp, r, a);
 }
 
-// Add c weights to the conductances in order.  Each conductance only sees its
-// own type's weights, in order, so selecting per element reproduces the
-// interleaved sequential sum; loads are batched ahead of the dependent adds.
+// Add the c weights sw[] (types sty[]) to the conductances x[ND..ND+2] in order.
+// Each conductance only sees its own type's weights, in order, so one thread per
+// type (lane 0 of warps 0-2) adding its type's weights reproduces the interleaved
+// sequential sum.  Thread 0 owns x; block-wide, with barriers.
 template <int ND>
-__device__ __forceinline__ void ordered_sum(float *x, const float *sw, const uint8_t *sty, uint32_t c) {
-    float ge = x[ND], gi = x[ND + 1], gn = x[ND + 2];
-    uint32_t a = 0;
-    for (; a + 8 <= c; a += 8) {
-        float w[8];
-        int t[8];
+__device__ __forceinline__ void wide_fold(WideSmem &S, float *x, uint32_t c) {
+    const int tid = threadIdx.x;
+    if (tid == 0) { S.g[0] = x[ND]; S.g[1] = x[ND + 1]; S.g[2] = x[ND + 2]; }
+    __syncthreads();
+    const int T = tid >> 5;
+    if ((tid & 31) == 0 && T < 3) {
+        float g = S.g[T];
+        uint32_t a = 0;
+        for (; a + 8 <= c; a += 8) {
+            float w[8];
+            int t[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) { w[u] = sw[a + u]; t[u] = sty[a + u]; }
+            for (int u = 0; u < 8; ++u) { w[u] = S.sw[a + u]; t[u] = S.sty[a + u]; }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            ge = (t[u] == 0) ? ge + w[u] : ge;
-            gi = (t[u] == 1) ? gi + w[u] : gi;
-            gn = (t[u] == 2) ? gn + w[u] : gn;
+            for (int u = 0; u < 8; ++u) g = ((t[u] < 2 ? t[u] : 2) == T) ? g + w[u] : g;
         }
+        for (; a < c; ++a) {
+            const int t = S.sty[a];
+            g = ((t < 2 ? t : 2) == T) ? g + S.sw[a] : g;
+        }
+        S.g[T] = g;
     }
-    for (; a < c; ++a) {
-        const float w = sw[a];
-        const int t = sty[a];
-        ge = (t == 0) ? ge + w : ge;
-        gi = (t == 1) ? gi + w : gi;
-        gn = (t == 2) ? gn + w : gn;
-    }
-    x[ND] = ge;
-    x[ND + 1] = gi;
-    x[ND + 2] = gn;
+    __syncthreads();
+    if (tid == 0) { x[ND] = S.g[0]; x[ND + 1] = S.g[1]; x[ND + 2] = S.g[2]; }
 }
 
 template <int KIND, int INTEG>
 __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
                                                    double push_inv_dt = 0.0) {
     constexpr int ND = Model<KIND>::ND;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, nt = blockDim.x;
     const int slot = (int)(k % N.R);
     const int64_t gi = P.first + i;
+    __syncthreads();  // the block's previous neuron is done with S
+    // every load that does not depend on another goes out first
     uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
     uint32_t c = *cp;
-    __syncthreads();
+    const uint32_t capg = N.cap[gi];
+    const int64_t rbase = N.cap_base[gi];
     float x[kMaxVars];
-    if (tid == 0) load_state<KIND>(P, i, x);
+    NeuronAux ax{-1, 0};
+    if (tid == 0) {
+        load_state<KIND>(P, i, x);
+        ax = load_aux<KIND, INTEG>(P, i);
+    }
     if (c) {
-        if (tid == 0) *cp = 0;
-        const uint32_t capg = N.cap[gi];
         if (c > capg) { if (tid == 0) atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
-        Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
-        if (c <= (uint32_t)kWideSmem) {
-            const Arrival *ord;
-            if (c <= (uint32_t)kRankSort) {
-                // rank sort: position of each arrival = number of arrivals before it in
-                // (time, synapse order, bucket index) order; one pass, all keys distinct
-                for (int a = tid; a < (int)c; a += blockDim.x) S.sbuf[a] = r[a];
-                __syncthreads();
-                for (int a = tid; a < (int)c; a += blockDim.x) {
-                    const Arrival v = S.sbuf[a];
-                    int rank = 0;
-                    for (int b = 0; b < (int)c; ++b) {
-                        const Arrival u = S.sbuf[b];
-                        rank += (arr_less(u, v) || (!arr_less(v, u) && b < a)) ? 1 : 0;
-                    }
-                    S.sorted[rank] = v;
-                }
-                __syncthreads();
-                ord = S.sorted;
-            } else {
-                int n2 = 1;
-                while (n2 < (int)c) n2 <<= 1;
-                for (int a = tid; a < n2; a += blockDim.x) {
-                    if (a < (int)c) S.sbuf[a] = r[a];
-                    else { S.sbuf[a].a = __longlong_as_double(0x7ff0000000000000LL); S.sbuf[a].spos = 0xffffffffu; S.sbuf[a].tpos = 0; }
-                }
-                __syncthreads();
-                for (int size = 2; size <= n2; size <<= 1)
-                    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                        for (int a = tid; a < n2; a += blockDim.x) {
-                            const int b = a ^ stride;
-                            if (b > a) {
-                                const bool up = ((a & size) == 0);
-                                const Arrival ea = S.sbuf[a], eb = S.sbuf[b];
-                                if (up ? arr_less(eb, ea) : arr_less(ea, eb)) { S.sbuf[a] = eb; S.sbuf[b] = ea; }
-                            }
-                        }
-                        __syncthreads();
-                    }
-                ord = S.sbuf;
+        Arrival *r = N.rec + (int64_t)slot * N.cap_total + rbase;
+        if (c <= (uint32_t)kRankSort) {
+            const bool own = tid < (int)c;
+            const bool ring = P.post_t != nullptr && !P.may_repeat;
+            Arrival v;
+            SynRec rec;
+            if (own) {
+                v = r[tid];
+                if (!P.may_repeat) rec = N.syn[v.tpos];  // in flight while the positions are counted
+                S.khi[tid] = time_key(v.a);
+                S.klo[tid] = v.spos;
+                S.rank[tid] = 0;
             }
+            if (ring) {  // the neuron's deferred post-synaptic spikes (slots past the count are unused)
+                for (int q = tid; q < kPostRing; q += nt) S.ring[q] = P.post_t[(int64_t)q * P.n + i];
+                if (tid == nt - 1) S.ring_n = P.post_n[i];
+            }
+            if (tid == 32) prefetch_l1(N.rule_par);
+            __syncthreads();
+            if (tid == 0) *cp = 0;
+            // position = arrivals before this one in (time, synapse order, bucket index)
+            // order; per threads share each arrival's comparisons
+            const int per = nt / (int)c;
+            if (tid < per * (int)c) {
+                const int e = tid % (int)c, s = tid / (int)c;
+                const int b0 = s * (int)c / per, b1 = (s + 1) * (int)c / per;
+                const unsigned long long kh = S.khi[e];
+                const uint32_t kl = S.klo[e];
+                uint32_t n = 0;
+#pragma unroll 4
+                for (int b = b0; b < b1; ++b) {
+                    const unsigned long long uh = S.khi[b];
+                    const uint32_t ul = S.klo[b];
+                    n += (uh < kh || (uh == kh && (ul < kl || (ul == kl && b < e)))) ? 1u : 0u;
+                }
+                if (per == 1) S.rank[e] = n;
+                else if (n) atomicAdd(&S.rank[e], n);
+            }
+            __syncthreads();
+            if (P.may_repeat) {
+                if (own) S.sbuf[S.rank[tid]] = v;
+                __syncthreads();
+                if (tid == 0)
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, S.sbuf[a], x);
+            } else {
+                if (own) {
+                    if (rec.rule >= 0) {
+                        if (ring) apply_pending(N, RingSmem{S.ring}, S.ring_n, rec);
+                        S.sw[S.rank[tid]] = rec.w;
+                        stdp_pre(N, v.tpos, rec, v.a);
+                    } else {
+                        S.sw[S.rank[tid]] = rec.w;
+                    }
+                    S.sty[S.rank[tid]] = rec.stype;
+                }
+                wide_fold<ND>(S, x, c);
+            }
+        } else if (c <= (uint32_t)kWideSmem) {
+            int n2 = 1;
+            while (n2 < (int)c) n2 <<= 1;
+            for (int a = tid; a < n2; a += nt) {
+                if (a < (int)c) S.sbuf[a] = r[a];
+                else { S.sbuf[a].a = __longlong_as_double(0x7ff0000000000000LL); S.sbuf[a].spos = 0xffffffffu; S.sbuf[a].tpos = 0; }
+            }
+            __syncthreads();
+            if (tid == 0) *cp = 0;
+            for (int size = 2; size <= n2; size <<= 1)
+                for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                    for (int a = tid; a < n2; a += nt) {
+                        const int b = a ^ stride;
+                        if (b > a) {
+                            const bool up = ((a & size) == 0);
+                            const Arrival ea = S.sbuf[a], eb = S.sbuf[b];
+                            if (up ? arr_less(eb, ea) : arr_less(ea, eb)) { S.sbuf[a] = eb; S.sbuf[b] = ea; }
+                        }
+                    }
+                    __syncthreads();
+                }
             if (P.may_repeat) {
                 if (tid == 0)
-                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, ord[a], x);
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, S.sbuf[a], x);
             } else {
-                for (int a = tid; a < (int)c; a += blockDim.x) {
-                    const Arrival v = ord[a];
+                for (int a = tid; a < (int)c; a += nt) {
+                    const Arrival v = S.sbuf[a];
                     float w_old;
                     int ty;
                     stdp_pre_gather(P, N, i, v.tpos, v.a, w_old, ty);
@@ -467,21 +564,25 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
                     S.sty[a] = (uint8_t)ty;
                 }
                 __syncthreads();
-                if (tid == 0) ordered_sum<ND>(x, S.sw, S.sty, c);
+                wide_fold<ND>(S, x, c);
             }
-        } else if (tid == 0) {
-            for (uint32_t a = 1; a < c; ++a) {  // rare: insertion sort in global memory
-                Arrival v = r[a];
-                int b = (int)a - 1;
-                while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
-                r[b + 1] = v;
+        } else {
+            __syncthreads();  // every thread has read the count before it is cleared
+            if (tid == 0) {
+                *cp = 0;
+                for (uint32_t a = 1; a < c; ++a) {  // rare: insertion sort in global memory
+                    Arrival v = r[a];
+                    int b = (int)a - 1;
+                    while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
+                    r[b + 1] = v;
+                }
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
             }
-            for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
         }
         if (tid == 0) atomicAdd(P.events, (unsigned long long)c);
     }
     if (tid == 0) {
-        const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x);
+        const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax);
         S.spiked = sp ? 1 : 0;
         if (sp && P.post_t) note_post_spike(P, N, i, k);
         store_state<KIND>(P, i, x);

@@ -74,3 +74,21 @@ def test_fp64_error_is_reported(oracle):
     rms = float(np.sqrt(np.mean((r["trace"][:, :, 0] - o64["trace"][:, :, 0]) ** 2)))
     print("V RMS vs FP64 oracle over 100 ms: %.3g mV" % rms)
     assert rms < 1e-2
+
+
+@pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "graphs"])
+def test_gpu_wide_fanin_matches_oracle(oracle, persistent):
+    """Block-per-neuron update at every arrival-count regime (tens of arrivals, up
+    to 256, up to 1024 and beyond in one step), with STDP on every delivered
+    synapse, deferred post-synaptic spikes, and a population whose input synapses
+    can deliver twice in one step: bit-exact against the oracle."""
+    from edlut_b200.configs import wide_fanin_network
+    net, t, c = wide_fanin_network()
+    first = sum(l.n for l in net.layers[:2])
+    trace = (400, first, 6)
+    o = oracle.run(net, t, c, 400, trace=trace)
+    r = run_gpu(net, t, c, 400, trace, persistent=persistent)
+    np.testing.assert_array_equal(r["spikes"], spike_pairs(o["spike_step"], o["spike_cell"]))
+    np.testing.assert_array_equal(r["trace"], o["trace"].astype(np.float32))
+    np.testing.assert_array_equal(r["w"], o["w_final"].astype(np.float32))
+    assert r["counters"]["events"] == o["n_events"]
