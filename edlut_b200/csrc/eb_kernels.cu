@@ -255,7 +255,7 @@ __device__ __forceinline__ void bucket_put(const NetDev &N, int64_t ka, double a
     const uint32_t tp = N.out_tpos[o];
     const uint32_t capg = N.cap[tg];
     const int64_t base = N.cap_base[tg];
-    const int slot = (int)(ka % N.R);
+    const int slot = (int)(ka & (N.R - 1));
     const uint32_t idx = atomicAdd(N.cnt + (int64_t)slot * N.n_neurons + tg, 1u);
     if (idx < capg) {
         Arrival v;
@@ -320,7 +320,7 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
         const int64_t gi = P.first + i;
         float x[kMaxVars];
         load_state<KIND>(P, i, x);
-        const int slot = (int)(k % N.R);
+        const int slot = (int)(k & (N.R - 1));
         uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
         c = *cp;
         if (c) {
@@ -457,7 +457,7 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
                                                    double push_inv_dt = 0.0) {
     constexpr int ND = Model<KIND>::ND;
     const int tid = threadIdx.x, nt = blockDim.x;
-    const int slot = (int)(k % N.R);
+    const int slot = (int)(k & (N.R - 1));
     const int64_t gi = P.first + i;
     __syncthreads();  // the block's previous neuron is done with S
     // every load that does not depend on another goes out first

@@ -262,9 +262,12 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         h_cap_base[i] = cap_total;
         cap_total += c;
     }
-    // delay ring: arrival at most ceil(max delay / dt) + 1 steps ahead
+    // delay ring: arrival at most ceil(max delay / dt) + 1 steps ahead; a power of
+    // two, so the kernels take the slot of step k as k & (R - 1)
     const double dmax = (double)max_units * 0.0001;
-    R = (int)std::ceil(dmax / dt_s) + 3;
+    const int r_min = (int)std::ceil(dmax / dt_s) + 3;
+    R = 1;
+    while (R < r_min) R <<= 1;
 
     int rc;
     cudaStream_t st = stream;

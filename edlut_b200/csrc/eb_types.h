@@ -86,7 +86,7 @@ struct PopDev {
 // Network-wide device pointers, passed by value to the kernels.
 struct NetDev {
     int64_t n_neurons;
-    int R;                       // delay-ring slots
+    int R;                       // delay-ring slots (a power of two)
     const int64_t *step;         // current step counter (steps completed)
     const double *tstep;         // update times t_k, k = 0..
     const double *tgen;          // Poisson generators' own update times (step 0.1f/1000 s)
