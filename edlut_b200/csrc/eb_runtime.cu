@@ -455,6 +455,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         p.push_threads = (int)std::min<int64_t>(256, std::max<int64_t>(32, (max_out + 31) / 32 * 32));
         D.may_repeat = in_from_inputs > 0 ? 1 : 0;
     }
+    plan_chains(out_ptr, h_out_tgt, h_out_units);
     if ((rc = seed_generators())) return rc;
     // dynamic state copied by eb_snapshot / eb_restore
     dyn.clear();
@@ -482,12 +483,12 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
             dyn.push_back({p.dev.post_flushed, sizeof(uint32_t) * (size_t)p.n});
         }
     }
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < std::max(4, (int)chain_pop.size() - 1); ++q) {
         cudaStream_t ss;
         CK(cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking));
         side.push_back(ss);
     }
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < std::max(8, (int)chain_pop.size()); ++q) {
         cudaEvent_t a, b;
         CK(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
@@ -790,12 +791,104 @@ int eb_ctx::setup_persistent() {
     return EB_OK;
 }
 
+// Chains of the captured graph: one per model population, one for all input
+// neurons (chain 0, so that its launch of step r is captured before the updates of
+// step r).  Population B's update at step k reads and clears bucket slot k; a
+// source chain A writes, at step j, arrivals for steps j + lo .. j + hi, lo and hi
+// bounding the arrival offsets of the delays from A to B with a step of margin for
+// rounding of the time grid.  So B(k) waits for A(k - lo) -- every arrival of step
+// k is in place -- and A(j) waits for B(j - (R - hi)) -- the slot it fills for
+// step j + hi has been cleared for its previous use, R steps before.  Everything
+// else a chain touches belongs to its own population (state, spike lists, the
+// target-major synapse records and the deferred post-synaptic rings), so the
+// chains need no other edge and the steps run exactly as in step order.
+void eb_ctx::plan_chains(const std::vector<int64_t> &out_ptr, const std::vector<uint32_t> &out_tgt,
+                         const std::vector<uint16_t> &out_units) {
+    chain_pop.clear();
+    chain_deps.clear();
+    std::vector<int> chain_of(pops.size(), -1);
+    if (has_inputs) chain_pop.push_back(-1);
+    for (size_t q = 0; q < pops.size(); ++q) {
+        if (pops[q].kind == KIND_INPUT) chain_of[q] = 0;
+        else { chain_of[q] = (int)chain_pop.size(); chain_pop.push_back((int)q); }
+    }
+    const int nc = (int)chain_pop.size();
+    std::vector<int64_t> umin((size_t)nc * nc, INT64_MAX), umax((size_t)nc * nc, -1);
+    for (int64_t i = 0; i < n_neurons; ++i) {
+        const int a = chain_of[pop_of[i]];
+        for (int64_t s = out_ptr[i]; s < out_ptr[i + 1]; ++s) {
+            const int b = chain_of[pop_of[out_tgt[s]]];
+            const size_t e = (size_t)a * nc + b;
+            umin[e] = std::min<int64_t>(umin[e], out_units[s]);
+            umax[e] = std::max<int64_t>(umax[e], out_units[s]);
+        }
+    }
+    chain_deps.assign(nc, {});
+    for (int a = 0; a < nc; ++a)
+        for (int b = 0; b < nc; ++b) {
+            const size_t e = (size_t)a * nc + b;
+            if (a == b || umax[e] < 0) continue;
+            const bool from_inputs = chain_pop[a] < 0;
+            // inputs of step j are the spikes of [t_{j-1}, t_j): one step earlier than a
+            // neuron's spike at t_j, so one step less of lower bound
+            const int lo = std::max(from_inputs ? 0 : 1,
+                                    (int)std::floor((double)umin[e] * 0.0001 / dt_s) - (from_inputs ? 2 : 1));
+            const int hi = (int)std::ceil((double)umax[e] * 0.0001 / dt_s) + 2;
+            chain_deps[b].push_back({a, lo});
+            chain_deps[a].push_back({b, R - hi});
+        }
+    chains_ok = nc >= 2 && nc <= 8;
+    for (auto &p : pops)
+        if (p.kind != KIND_INPUT && p.has_plastic_in && !p.dev.post_t) chains_ok = false;  // eager post phase
+    for (auto &d : chain_deps)
+        for (auto &x : d)
+            if (x.lag < 0 || (x.lag == 0 && chain_pop[x.other] >= 0)) chains_ok = false;
+}
+
+// K steps as per-population chains (see plan_chains), joined at the end.
+void eb_ctx::enqueue_chains(int K) {
+    const int nc = (int)chain_pop.size();
+    while ((int)chain_ev.size() < nc * K) {
+        cudaEvent_t e;
+        cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+        chain_ev.push_back(e);
+    }
+    auto ev = [&](int c, int r) { return chain_ev[(size_t)c * K + r]; };
+    auto strm = [&](int c) { return c == 0 ? stream : side[c - 1]; };
+    const double inv_dt = 1.0 / dt_s;
+    cudaEventRecord(fork_ev[0], stream);
+    for (int c = 1; c < nc; ++c) cudaStreamWaitEvent(strm(c), fork_ev[0], 0);
+    for (int r = 0; r < K; ++r)
+        for (int c = 0; c < nc; ++c) {
+            cudaStream_t s = strm(c);
+            for (auto &d : chain_deps[c]) {
+                const int x = r - d.lag;
+                if (x >= 0) cudaStreamWaitEvent(s, ev(d.other, x), 0);
+            }
+            const int q = chain_pop[c];
+            if (q < 0) {
+                launch_input_push(net, r, inv_dt, 148 * 4, input_threads, s);
+            } else {
+                const double push_inv_dt = pops[q].has_out ? inv_dt : 0.0;
+                launch_update(pops[q].dev, net, r, push_inv_dt, s);
+            }
+            enq_count++;
+            cudaEventRecord(ev(c, r), s);
+        }
+    for (int c = 1; c < nc; ++c) {
+        cudaEventRecord(join_ev[c], strm(c));
+        cudaStreamWaitEvent(stream, join_ev[c], 0);
+    }
+}
+
 int eb_ctx::build_graph(int K) {
     if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     enq_count = 0;
-    for (int r = 0; r < K; ++r) enqueue_step(r);
+    if (chains_ok && chains_enabled) enqueue_chains(K);
+    else
+        for (int r = 0; r < K; ++r) enqueue_step(r);
     if (lazy_post) enqueue_flush();
     graph_kernels = enq_count + 1;
     launch_advance(d_step, K, stream);
@@ -964,6 +1057,7 @@ int eb_ctx::restore(int slot) {
 eb_ctx::~eb_ctx() {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     for (auto s : side) cudaStreamDestroy(s);
+    for (auto e : chain_ev) cudaEventDestroy(e);
     for (auto e : fork_ev) cudaEventDestroy(e);
     for (auto e : join_ev) cudaEventDestroy(e);
     for (auto &r : prof_pending) { ev_pool.push_back(r.a); ev_pool.push_back(r.b); }

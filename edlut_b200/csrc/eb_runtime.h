@@ -74,6 +74,12 @@ struct eb_ctx {
     // side streams and events for the parallel branches of a step
     std::vector<cudaStream_t> side;
     std::vector<cudaEvent_t> fork_ev, join_ev;
+    // captured graphs as one kernel chain per population (plan_chains)
+    struct ChainDep { int other, lag; };       // wait for chain `other` at step r - lag
+    std::vector<int> chain_pop;                // chain -> population (-1: all input neurons)
+    std::vector<std::vector<ChainDep>> chain_deps;
+    std::vector<cudaEvent_t> chain_ev;         // [chain][step of the graph]
+    bool chains_ok = false, chains_enabled = true;
     // time grid and inputs
     std::vector<double> t_host;
     double *d_tstep = nullptr;
@@ -132,6 +138,9 @@ struct eb_ctx {
     void prof_end(int kind, int pop, cudaEvent_t a);
     int prof_collect();
     int build_graph(int K);
+    void plan_chains(const std::vector<int64_t> &out_ptr, const std::vector<uint32_t> &out_tgt,
+                     const std::vector<uint16_t> &out_units);
+    void enqueue_chains(int K);
     int setup_persistent();
     int seed_generators();
     void enqueue_flush();
