@@ -84,28 +84,63 @@ __device__ __forceinline__ void stdp_post(const NetDev &N, SynRec &r, double t) 
 // the same updates in the same order as at each spike, only later.  Every spike
 // of the ring is at most the arrival time being processed (spikes of this step
 // are recorded after the fold), and at an equal time the spike came first.
-// The ring holds the target's last kPostRing spike times, slot = count % kPostRing,
-// in global memory (RingGlobal) or staged in shared memory (RingSmem).
+// The ring holds the target's last kPostRing spike times (slot = spike number %
+// kPostRing) and, when the population has one plastic rule, the trace decay
+// factors of the interval ending at each spike; in global memory (RingGlobal) or
+// staged in shared memory (RingSmem).
 struct RingGlobal {
-    const double *t;
-    int64_t n, i;
-    __device__ double operator()(uint32_t slot) const { return t[(int64_t)slot * n + i]; }
+    const double *t;     // the neuron's kPostRing times
+    const DecayPair *f;  // and factors
+    __device__ double time(uint32_t slot) const { return t[slot]; }
+    __device__ DecayPair fac(uint32_t slot) const { return f[slot]; }
 };
 struct RingSmem {
     const double *t;
-    __device__ double operator()(uint32_t slot) const { return t[slot]; }
+    const DecayPair *f;
+    __device__ double time(uint32_t slot) const { return t[slot]; }
+    __device__ DecayPair fac(uint32_t slot) const { return f[slot]; }
 };
 
+// Apply to r the ring's spikes after r.last, oldest first, as stdp_post would one
+// by one.  Spike times increase with the spike number, so the first pending one
+// is found by bisection.  After the first, r.last is the previous spike, so each
+// update's elapsed time -- and its two table lookups -- are the interval's: they
+// come from the factor ring when r follows the ring's rule (rule >= 0).
 template <class Ring>
-__device__ __forceinline__ void apply_pending(const NetDev &N, Ring ring, uint32_t c, SynRec &r) {
+__device__ __forceinline__ void apply_pending(const NetDev &N, const Ring &ring, uint32_t c, int rule, SynRec &r) {
     const uint32_t lim = c < (uint32_t)kPostRing ? c : (uint32_t)kPostRing;
-    uint32_t np = 0;
-    while (np < lim && ring((c - 1 - np) % kPostRing) > r.last) ++np;
-    for (uint32_t q = np; q > 0; --q) stdp_post(N, r, ring((c - q) % kPostRing));
+    uint32_t lo = c - lim, hi = c;  // first spike number in [lo, hi) with time > r.last
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (ring.time(mid % kPostRing) > r.last) hi = mid;
+        else lo = mid + 1;
+    }
+    if (lo == c) return;
+    stdp_post(N, r, ring.time(lo % kPostRing));
+    if (rule >= 0 && r.rule == rule) {
+        const float a = N.rule_par[rule * 6];
+        float w = r.w, pre = r.pre, post = r.post;
+        for (uint32_t q = lo + 1; q < c; ++q) {
+            const DecayPair f = ring.fac(q % kPostRing);
+            pre = pre * f.pre;
+            post = post * f.post;
+            post += 1.0f;
+            w = w + a * pre;
+            if (w > r.maxw) w = r.maxw; else if (w < 0.0f) w = 0.0f;
+        }
+        r.w = w;
+        r.pre = pre;
+        r.post = post;
+        r.last = ring.time((c - 1) % kPostRing);
+    } else {
+        for (uint32_t q = lo + 1; q < c; ++q) stdp_post(N, r, ring.time(q % kPostRing));
+    }
 }
 
 __device__ __forceinline__ void apply_pending_post(const PopDev &P, const NetDev &N, int64_t i, SynRec &r) {
-    apply_pending(N, RingGlobal{P.post_t, P.n, i}, P.post_n[i], r);
+    const int64_t o = i * kPostRing;
+    apply_pending(N, RingGlobal{P.post_t + o, P.post_f ? P.post_f + o : nullptr}, P.post_n[i],
+                  P.post_f ? P.post_rule : -1, r);
 }
 
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
@@ -128,10 +163,19 @@ __device__ __forceinline__ void apply_arrival(const PopDev &P, const NetDev &N, 
     if (s.rule >= 0) stdp_pre(N, tp, s, r.a);
 }
 
-// Record a spike of neuron i at step k for deferred post-synaptic STDP.
+// Record a spike of neuron i at step k for deferred post-synaptic STDP, with the
+// decay factors of the interval from its previous spike (stdp_post's lookups for
+// a synapse last updated at that spike).
 __device__ __forceinline__ void note_post_spike(const PopDev &P, const NetDev &N, int64_t i, int64_t k) {
     const uint32_t c = P.post_n[i];
-    P.post_t[(int64_t)(c % kPostRing) * P.n + i] = N.tstep[k];
+    const double t = N.tstep[k];
+    const int64_t o = i * kPostRing + c % kPostRing;
+    if (P.post_f && c > 0) {
+        const float *rp = N.rule_par + P.post_rule * 6;
+        const float el = (float)(t - P.post_t[i * kPostRing + (c - 1) % kPostRing]);
+        P.post_f[o] = DecayPair{expt_net(N, -el * rp[4]), expt_net(N, -el * rp[5])};
+    }
+    P.post_t[o] = t;
     P.post_n[i] = c + 1;
 }
 
@@ -166,9 +210,16 @@ __device__ __forceinline__ NeuronAux load_aux(const PopDev &P, int64_t i) {
     return a;
 }
 
-// Advance one neuron (after its arrivals were folded); returns spike flag.
 template <int KIND, int INTEG>
-__device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N, int64_t i, float *x, NeuronAux ax) {
+__device__ __forceinline__ void store_aux(const PopDev &P, int64_t i, const NeuronAux &a) {
+    if (KIND == KIND_LIF) P.refr[i] = a.refr;
+    if (INTEG == INTEG_BDF) P.bdf_state[i] = (int8_t)a.bst;
+}
+
+// Advance one neuron (after its arrivals were folded); returns spike flag.  The
+// integer state is updated in ax (store_aux writes it back).
+template <int KIND, int INTEG>
+__device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N, int64_t i, float *x, NeuronAux &ax) {
     constexpr int NV = Model<KIND>::NV;
     int refr = ax.refr;
     int bst = ax.bst;
@@ -186,14 +237,9 @@ __device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N,
 #pragma unroll
         for (int v = 0; v < NV; ++v) x[v] = P.init[v];
     }
-    if (KIND == KIND_LIF) P.refr[i] = refr;
-    if (INTEG == INTEG_BDF) P.bdf_state[i] = (int8_t)bst;
+    ax.refr = refr;
+    ax.bst = bst;
     return sp;
-}
-
-template <int KIND, int INTEG>
-__device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N, int64_t i, float *x) {
-    return advance_neuron<KIND, INTEG>(P, N, i, x, load_aux<KIND, INTEG>(P, i));
 }
 
 __device__ __forceinline__ void record_trace(const PopDev &P, const NetDev &N, int64_t k, int64_t gi, const float *x, int nv) {
@@ -204,9 +250,11 @@ __device__ __forceinline__ void record_trace(const PopDev &P, const NetDev &N, i
     for (int v = 0; v < nv; ++v) o[v] = x[v];
 }
 
-// Warp-aggregated append of the spiking lanes to the population spike list and
-// to the recording buffer.
-__device__ __forceinline__ void compact_spikes(const PopDev &P, const NetDev &N, int64_t k, int64_t i, bool sp) {
+// Warp-aggregated append of the spiking lanes to the population spike list (when
+// list is set: launches of one step, whose list the eager post-synaptic and
+// separate fan-out kernels read) and to the recording buffer.
+__device__ __forceinline__ void compact_spikes(const PopDev &P, const NetDev &N, int64_t k, int64_t i, bool sp,
+                                               bool list = true) {
     const unsigned full = 0xffffffffu;
     const unsigned m = __ballot_sync(full, sp);
     if (!m) return;
@@ -216,15 +264,19 @@ __device__ __forceinline__ void compact_spikes(const PopDev &P, const NetDev &N,
     uint32_t base = 0;
     unsigned long long rbase = 0;
     if (lane == leader) {
-        base = atomicAdd(&P.spk_count[k & 1], (uint32_t)__popc(m));
+        if (list) base = atomicAdd(&P.spk_count[k & 1], (uint32_t)__popc(m));
         if (N.rec_buf) rbase = atomicAdd(N.rec_count, (unsigned long long)__popc(m));
     }
     base = __shfl_sync(full, base, leader);
     rbase = __shfl_sync(full, rbase, leader);
     if (sp) {
         const uint32_t o = base + __popc(below);
-        if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
-        else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
+        if (!list) {
+        } else if (o < (uint32_t)P.n) {
+            P.spk[o] = (uint32_t)i;
+        } else {
+            atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
+        }
         if (N.rec_buf) {
             const unsigned long long ro = rbase + __popc(below);
             if (ro < (unsigned long long)N.rec_cap)
@@ -308,18 +360,16 @@ __device__ __forceinline__ void warp_push(const PopDev &P, const NetDev &N, int6
 constexpr int kLocalSort = 16;
 constexpr int kNarrowTile = 256;
 
+// One step of neuron i (lanes with active unset only join the warp collectives);
+// x and ax hold its state, loaded and stored by the caller.
 template <int KIND, int INTEG>
-__device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev &N, int64_t k, int64_t tile,
-                                                   double push_inv_dt = 0.0) {
+__device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, int64_t k, int64_t i, bool active,
+                                            float *x, NeuronAux &ax, bool list, double push_inv_dt) {
     constexpr int ND = Model<KIND>::ND;
-    const int64_t i = tile * kNarrowTile + threadIdx.x;
-    const bool active = i < P.n;
     bool sp = false;
     uint32_t c = 0;
     if (active) {
         const int64_t gi = P.first + i;
-        float x[kMaxVars];
-        load_state<KIND>(P, i, x);
         const int slot = (int)(k & (N.R - 1));
         uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
         c = *cp;
@@ -349,26 +399,62 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
                 for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
             }
         }
-        sp = advance_neuron<KIND, INTEG>(P, N, i, x);
-        store_state<KIND>(P, i, x);
+        sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax);
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
         if (sp && P.post_t) note_post_spike(P, N, i, k);
     }
     // delivered-event counter: one atomic per warp
-    unsigned long long cw = c;
+    if (__any_sync(0xffffffffu, c != 0)) {
+        unsigned long long cw = c;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cw += __shfl_down_sync(0xffffffffu, cw, o);
-    if ((threadIdx.x & 31) == 0 && cw) atomicAdd(P.events, cw);
-    compact_spikes(P, N, k, i, sp);
+        for (int o = 16; o > 0; o >>= 1) cw += __shfl_down_sync(0xffffffffu, cw, o);
+        if ((threadIdx.x & 31) == 0 && cw) atomicAdd(P.events, cw);
+    }
+    compact_spikes(P, N, k, i, sp, list);
     if (push_inv_dt > 0.0) warp_push(P, N, k, i, sp, push_inv_dt);
 }
 
-// push_inv_dt > 0: also fan out this step's spikes (1 / step, for arrival_step).
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kNarrowTile) k_update_narrow(PopDev P, NetDev N, int rel, double push_inv_dt) {
+__device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev &N, int64_t k, int64_t tile,
+                                                   double push_inv_dt = 0.0) {
+    const int64_t i = tile * kNarrowTile + threadIdx.x;
+    const bool active = i < P.n;
+    float x[kMaxVars];
+    NeuronAux ax{-1, 0};
+    if (active) {
+        load_state<KIND>(P, i, x);
+        ax = load_aux<KIND, INTEG>(P, i);
+    }
+    narrow_step<KIND, INTEG>(P, N, k, i, active, x, ax, true, push_inv_dt);
+    if (active) {
+        store_state<KIND>(P, i, x);
+        store_aux<KIND, INTEG>(P, i, ax);
+    }
+}
+
+// Steps k .. k+nsteps-1 of one tile, the state in registers between them.  Only a
+// launch of one step keeps the population spike list (with several, no kernel
+// reads it: fan-out is done here and post-synaptic STDP is deferred).
+// push_inv_dt > 0: also fan out the spikes (1 / step, for arrival_step).
+template <int KIND, int INTEG>
+__global__ void __launch_bounds__(kNarrowTile) k_update_narrow(PopDev P, NetDev N, int rel, int nsteps,
+                                                                double push_inv_dt) {
     const int64_t k = cur_step(N, rel);
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
-    update_narrow_tile<KIND, INTEG>(P, N, k, blockIdx.x, push_inv_dt);
+    const bool list = nsteps == 1;
+    if (list && blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
+    const int64_t i = (int64_t)blockIdx.x * kNarrowTile + threadIdx.x;
+    const bool active = i < P.n;
+    float x[kMaxVars];
+    NeuronAux ax{-1, 0};
+    if (active) {
+        load_state<KIND>(P, i, x);
+        ax = load_aux<KIND, INTEG>(P, i);
+    }
+    for (int s = 0; s < nsteps; ++s) narrow_step<KIND, INTEG>(P, N, k + s, i, active, x, ax, list, push_inv_dt);
+    if (active) {
+        store_state<KIND>(P, i, x);
+        store_aux<KIND, INTEG>(P, i, ax);
+    }
 }
 
 // ------------------------------------------------------------- wide update --
@@ -398,6 +484,7 @@ struct WideSmem {
     uint32_t klo[kRankSort];            // synapse order
     uint32_t rank[kRankSort];           // delivery position
     double ring[kPostRing];             // the neuron's deferred post-synaptic spike times
+    DecayPair ring_f[kPostRing];           // and the decay factors of their intervals
     Arrival sbuf[kWideSmem];
     float sw[kWideSmem];
     uint8_t sty[kWideSmem];
@@ -452,9 +539,11 @@ __device__ __forceinline__ void wide_fold(WideSmem &S, float *x, uint32_t c) {
     if (tid == 0) { x[ND] = S.g[0]; x[ND + 1] = S.g[1]; x[ND + 2] = S.g[2]; }
 }
 
+// One step of wide neuron i by the whole block; thread 0 holds its state in x and
+// ax (loaded and stored by the caller).
 template <int KIND, int INTEG>
-__device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
-                                                   double push_inv_dt = 0.0) {
+__device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
+                                          float *x, NeuronAux &ax, bool list, double push_inv_dt) {
     constexpr int ND = Model<KIND>::ND;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int slot = (int)(k & (N.R - 1));
@@ -465,12 +554,6 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
     uint32_t c = *cp;
     const uint32_t capg = N.cap[gi];
     const int64_t rbase = N.cap_base[gi];
-    float x[kMaxVars];
-    NeuronAux ax{-1, 0};
-    if (tid == 0) {
-        load_state<KIND>(P, i, x);
-        ax = load_aux<KIND, INTEG>(P, i);
-    }
     if (c) {
         if (c > capg) { if (tid == 0) atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
         Arrival *r = N.rec + (int64_t)slot * N.cap_total + rbase;
@@ -487,7 +570,10 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
                 S.rank[tid] = 0;
             }
             if (ring) {  // the neuron's deferred post-synaptic spikes (slots past the count are unused)
-                for (int q = tid; q < kPostRing; q += nt) S.ring[q] = P.post_t[(int64_t)q * P.n + i];
+                for (int q = tid; q < kPostRing; q += nt) {
+                    S.ring[q] = P.post_t[i * kPostRing + q];
+                    if (P.post_f) S.ring_f[q] = P.post_f[i * kPostRing + q];
+                }
                 if (tid == nt - 1) S.ring_n = P.post_n[i];
             }
             if (tid == 32) prefetch_l1(N.rule_par);
@@ -520,7 +606,7 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
             } else {
                 if (own) {
                     if (rec.rule >= 0) {
-                        if (ring) apply_pending(N, RingSmem{S.ring}, S.ring_n, rec);
+                        if (ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, P.post_f ? P.post_rule : -1, rec);
                         S.sw[S.rank[tid]] = rec.w;
                         stdp_pre(N, v.tpos, rec, v.a);
                     } else {
@@ -585,12 +671,13 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
         const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax);
         S.spiked = sp ? 1 : 0;
         if (sp && P.post_t) note_post_spike(P, N, i, k);
-        store_state<KIND>(P, i, x);
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
         if (sp) {
-            const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
-            if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
-            else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
+            if (list) {
+                const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
+                if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
+                else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
+            }
             if (N.rec_buf) {
                 const unsigned long long ro = atomicAdd(N.rec_count, 1ull);
                 if (ro < (unsigned long long)N.rec_cap)
@@ -604,11 +691,42 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
 }
 
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel, double push_inv_dt) {
+__device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
+                                                   double push_inv_dt = 0.0) {
+    float x[kMaxVars];
+    NeuronAux ax{-1, 0};
+    if (threadIdx.x == 0) {
+        load_state<KIND>(P, i, x);
+        ax = load_aux<KIND, INTEG>(P, i);
+    }
+    wide_step<KIND, INTEG>(P, N, k, i, S, x, ax, true, push_inv_dt);
+    if (threadIdx.x == 0) {
+        store_state<KIND>(P, i, x);
+        store_aux<KIND, INTEG>(P, i, ax);
+    }
+}
+
+// Steps k .. k+nsteps-1 of the block's neurons (spike list as in k_update_narrow).
+template <int KIND, int INTEG>
+__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
+                                                              double push_inv_dt) {
     __shared__ WideSmem S;
     const int64_t k = cur_step(N, rel);
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
-    for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) update_wide_neuron<KIND, INTEG>(P, N, k, i, S, push_inv_dt);
+    const bool list = nsteps == 1;
+    if (list && blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
+    for (int64_t i = blockIdx.x; i < P.n; i += gridDim.x) {
+        float x[kMaxVars];
+        NeuronAux ax{-1, 0};
+        if (threadIdx.x == 0) {
+            load_state<KIND>(P, i, x);
+            ax = load_aux<KIND, INTEG>(P, i);
+        }
+        for (int s = 0; s < nsteps; ++s) wide_step<KIND, INTEG>(P, N, k + s, i, S, x, ax, list, push_inv_dt);
+        if (threadIdx.x == 0) {
+            store_state<KIND>(P, i, x);
+            store_aux<KIND, INTEG>(P, i, ax);
+        }
+    }
 }
 
 // PoissonGeneratorDeviceVector::UpdateState (src/neuron_model/PoissonGeneratorDeviceVector.cpp:56-70):
@@ -617,22 +735,25 @@ __global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N
 // (include/simulation/RandomGenerator.h:91-107) -- and fires when
 // frequency * step > frand.  The low 31 bits of the product only depend on its low
 // 32 bits, so 32-bit arithmetic gives the reference's sequence.
-__global__ void __launch_bounds__(256) k_update_poisson(PopDev P, NetDev N, int rel, double push_inv_dt) {
-    const int64_t k = cur_step(N, rel);
-    if (blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
+__global__ void __launch_bounds__(256) k_update_poisson(PopDev P, NetDev N, int rel, int nsteps, double push_inv_dt) {
+    const int64_t k0 = cur_step(N, rel);
+    const bool list = nsteps == 1;
+    if (list && blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k0 + 1) & 1] = 0;
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    bool sp = false;
-    if (i < P.n) {
-        const double thr = P.pthr[i];
+    const double thr = i < P.n ? P.pthr[i] : 0.0;
+    uint32_t x = i < P.n ? P.lcg[i] : 0u;
+    for (int s = 0; s < nsteps; ++s) {
+        const int64_t k = k0 + s;
+        bool sp = false;
         if (thr > 0.0) {
-            const uint32_t x = (P.lcg[i] * 1103515245u + 12345u) & 0x7fffffffu;
-            P.lcg[i] = x;
+            x = (x * 1103515245u + 12345u) & 0x7fffffffu;
             const float r = (float)x / (float)2147483647;
             sp = thr > (double)r;
         }
+        compact_spikes(P, N, k, i, sp, list);
+        if (push_inv_dt > 0.0) warp_push(P, N, k, i, sp, push_inv_dt);
     }
-    compact_spikes(P, N, k, i, sp);
-    if (push_inv_dt > 0.0) warp_push(P, N, k, i, sp, push_inv_dt);
+    if (i < P.n && thr > 0.0) P.lcg[i] = x;
 }
 
 // ------------------------------------------------------------ spike fan-out --
@@ -682,10 +803,14 @@ __global__ void __launch_bounds__(256) k_push(PopDev P, NetDev N, int rel, doubl
     for (int64_t s = blockIdx.x; s < ns; s += gridDim.x) push_spike(P, N, k, s, inv_dt);
 }
 
-__global__ void __launch_bounds__(256) k_input_push(NetDev N, int rel, double inv_dt) {
-    const int64_t k = cur_step(N, rel);
-    const int64_t q0 = N.in_start[k], q1 = N.in_start[k + 1];
-    for (int64_t q = q0 + blockIdx.x; q < q1; q += gridDim.x) input_spike(N, k, q, inv_dt);
+// Input spikes of steps k .. k+nsteps-1 (their deliveries are independent).
+__global__ void __launch_bounds__(256) k_input_push(NetDev N, int rel, int nsteps, double inv_dt) {
+    const int64_t k0 = cur_step(N, rel);
+    for (int s = 0; s < nsteps; ++s) {
+        const int64_t k = k0 + s;
+        const int64_t q0 = N.in_start[k], q1 = N.in_start[k + 1];
+        for (int64_t q = q0 + blockIdx.x; q < q1; q += gridDim.x) input_spike(N, k, q, inv_dt);
+    }
 }
 
 __global__ void __launch_bounds__(256) k_post_stdp(PopDev P, NetDev N, int rel, int max_chunks) {
@@ -953,33 +1078,35 @@ __global__ void k_advance(int64_t *step, int K) { *step += K; }
 
 // ------------------------------------------------------------------ launch --
 template <int KIND, int INTEG>
-static void launch_update_t(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st) {
+static void launch_update_t(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st) {
     if (P.wide) {
         const int blocks = (int)std::min<int64_t>(P.n, 148 * 8);
-        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, 0, st>>>(P, N, rel, push_inv_dt);
+        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
     } else {
         const int blocks = (int)((P.n + 255) / 256);
-        k_update_narrow<KIND, INTEG><<<blocks, 256, 0, st>>>(P, N, rel, push_inv_dt);
+        k_update_narrow<KIND, INTEG><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
     }
 }
 
 template <int KIND>
-static void launch_update_k(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st) {
+static void launch_update_k(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st) {
     switch (P.integ) {
-    case INTEG_EULER: launch_update_t<KIND, INTEG_EULER>(P, N, rel, push_inv_dt, st); break;
-    case INTEG_RK2: launch_update_t<KIND, INTEG_RK2>(P, N, rel, push_inv_dt, st); break;
-    case INTEG_RK4: launch_update_t<KIND, INTEG_RK4>(P, N, rel, push_inv_dt, st); break;
-    default: launch_update_t<KIND, INTEG_BDF>(P, N, rel, push_inv_dt, st); break;
+    case INTEG_EULER: launch_update_t<KIND, INTEG_EULER>(P, N, rel, nsteps, push_inv_dt, st); break;
+    case INTEG_RK2: launch_update_t<KIND, INTEG_RK2>(P, N, rel, nsteps, push_inv_dt, st); break;
+    case INTEG_RK4: launch_update_t<KIND, INTEG_RK4>(P, N, rel, nsteps, push_inv_dt, st); break;
+    default: launch_update_t<KIND, INTEG_BDF>(P, N, rel, nsteps, push_inv_dt, st); break;
     }
 }
 
-void launch_update(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st) {
+void launch_update(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st) {
     if (P.n <= 0) return;
     switch (P.kind) {
-    case KIND_LIF: launch_update_k<KIND_LIF>(P, N, rel, push_inv_dt, st); break;
-    case KIND_ADEX: launch_update_k<KIND_ADEX>(P, N, rel, push_inv_dt, st); break;
-    case KIND_HH: launch_update_k<KIND_HH>(P, N, rel, push_inv_dt, st); break;
-    case KIND_POISSON: k_update_poisson<<<(unsigned)((P.n + 255) / 256), 256, 0, st>>>(P, N, rel, push_inv_dt); break;
+    case KIND_LIF: launch_update_k<KIND_LIF>(P, N, rel, nsteps, push_inv_dt, st); break;
+    case KIND_ADEX: launch_update_k<KIND_ADEX>(P, N, rel, nsteps, push_inv_dt, st); break;
+    case KIND_HH: launch_update_k<KIND_HH>(P, N, rel, nsteps, push_inv_dt, st); break;
+    case KIND_POISSON:
+        k_update_poisson<<<(unsigned)((P.n + 255) / 256), 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        break;
     default: break;
     }
 }
@@ -988,8 +1115,8 @@ void launch_push(const PopDev &P, const NetDev &N, int rel, double inv_dt, int b
     k_push<<<blocks, threads, 0, st>>>(P, N, rel, inv_dt);
 }
 
-void launch_input_push(const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st) {
-    k_input_push<<<blocks, threads, 0, st>>>(N, rel, inv_dt);
+void launch_input_push(const NetDev &N, int rel, int nsteps, double inv_dt, int blocks, int threads, cudaStream_t st) {
+    k_input_push<<<blocks, threads, 0, st>>>(N, rel, nsteps, inv_dt);
 }
 
 void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks, int blocks, cudaStream_t st) {
@@ -999,16 +1126,43 @@ void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks,
 // Bring every plastic synapse onto the population up to date with its target's
 // deferred post-synaptic spikes: items are (neuron, chunk of kPostThreads plastic
 // synapses), neurons without spikes since the last flush skipped.
-__global__ void __launch_bounds__(kPostThreads) k_flush_post(PopDev P, NetDev N, int max_chunks) {
+// Only neurons with more than keep pending spikes are brought up to date.  Items
+// are (neuron, chunk of kPostThreads plastic synapses); each block takes a
+// contiguous run of them, so it reads a neuron's count once and stages its ring in
+// shared memory once for all the chunks it takes of it.
+__global__ void __launch_bounds__(kPostThreads) k_flush_post(PopDev P, NetDev N, int max_chunks, uint32_t keep) {
+    __shared__ double ring[kPostRing];
+    __shared__ DecayPair fac[kPostRing];
+    __shared__ uint32_t s_c;
+    __shared__ int s_go;
     const int64_t items = P.n * (int64_t)max_chunks;
-    for (int64_t item = blockIdx.x; item < items; item += gridDim.x) {
+    const int64_t per = (items + gridDim.x - 1) / gridDim.x;
+    const int64_t it0 = (int64_t)blockIdx.x * per, it1 = min(items, it0 + per);
+    const int rule = P.post_f ? P.post_rule : -1;
+    int64_t cur = -1;
+    for (int64_t item = it0; item < it1; ++item) {
         const int64_t i = item / max_chunks, ch = item % max_chunks;
-        if (P.post_n[i] == P.post_flushed[i]) continue;
+        if (i != cur) {
+            __syncthreads();  // the block is done with the previous neuron's ring
+            if (threadIdx.x == 0) {
+                s_c = P.post_n[i];
+                s_go = s_c - P.post_flushed[i] > keep;
+            }
+            __syncthreads();
+            if (s_go)
+                for (int q = threadIdx.x; q < kPostRing; q += blockDim.x) {
+                    ring[q] = P.post_t[i * kPostRing + q];
+                    if (P.post_f) fac[q] = P.post_f[i * kPostRing + q];
+                }
+            __syncthreads();
+            cur = i;
+        }
+        if (!s_go) continue;
         const int64_t t = P.first + i;
         const int64_t tp = N.in_ptr[t] + ch * kPostThreads + threadIdx.x;
         if (tp >= N.plastic_end[t]) continue;
         SynRec r = N.syn[tp];
-        apply_pending_post(P, N, i, r);
+        apply_pending(N, RingSmem{ring, fac}, s_c, rule, r);
         SynRec *o = N.syn + tp;
         o->w = r.w;
         o->pre = r.pre;
@@ -1017,14 +1171,14 @@ __global__ void __launch_bounds__(kPostThreads) k_flush_post(PopDev P, NetDev N,
     }
 }
 
-__global__ void k_flush_mark(PopDev P) {
+__global__ void k_flush_mark(PopDev P, uint32_t keep) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x)
-        P.post_flushed[i] = P.post_n[i];
+        if (P.post_n[i] - P.post_flushed[i] > keep) P.post_flushed[i] = P.post_n[i];
 }
 
-void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, int blocks, cudaStream_t st) {
-    k_flush_post<<<blocks, kPostThreads, 0, st>>>(P, N, max_chunks);
-    k_flush_mark<<<(unsigned)std::min<int64_t>((P.n + 255) / 256, 1184), 256, 0, st>>>(P);
+void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, uint32_t keep, int blocks, cudaStream_t st) {
+    k_flush_post<<<blocks, kPostThreads, 0, st>>>(P, N, max_chunks, keep);
+    k_flush_mark<<<(unsigned)std::min<int64_t>((P.n + 255) / 256, 1184), 256, 0, st>>>(P, keep);
 }
 
 void launch_advance(int64_t *step, int K, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(step, K); }

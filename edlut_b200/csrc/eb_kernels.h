@@ -4,14 +4,18 @@
 #include "eb_types.h"
 
 namespace eb {
-// push_inv_dt > 0: the update kernel also fans out the step's spikes (no launch_push).
-void launch_update(const PopDev &P, const NetDev &N, int rel, double push_inv_dt, cudaStream_t st);
+// Steps rel+1 .. rel+nsteps after the device step counter.  push_inv_dt > 0: the
+// update kernel also fans out the spikes (no launch_push).  With nsteps > 1 the
+// population spike list is not kept (the eager post-synaptic and separate fan-out
+// kernels cannot follow such a launch).
+void launch_update(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st);
 constexpr int kPostThreads = 256;  // plastic synapses per post-STDP work item
 void launch_push(const PopDev &P, const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st);
-void launch_input_push(const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st);
+void launch_input_push(const NetDev &N, int rel, int nsteps, double inv_dt, int blocks, int threads, cudaStream_t st);
 void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks, int blocks, cudaStream_t st);
-// Deferred post-synaptic STDP: apply the spikes noted since the last flush (2 launches).
-void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, int blocks, cudaStream_t st);
+// Deferred post-synaptic STDP: apply the spikes noted since the last flush to the
+// synapses of every neuron with more than keep of them (2 launches).
+void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, uint32_t keep, int blocks, cudaStream_t st);
 void launch_advance(int64_t *step, int K, cudaStream_t st);
 
 constexpr int kMaxPersistPops = 16;

@@ -262,10 +262,12 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         h_cap_base[i] = cap_total;
         cap_total += c;
     }
-    // delay ring: arrival at most ceil(max delay / dt) + 1 steps ahead; a power of
-    // two, so the kernels take the slot of step k as k & (R - 1)
+    // delay ring: arrival at most ceil(max delay / dt) + 1 steps ahead, plus
+    // kMaxFuse slots so that a launch can run that many steps of a population
+    // (see plan_chains); a power of two, so the kernels take the slot of step k as
+    // k & (R - 1)
     const double dmax = (double)max_units * 0.0001;
-    const int r_min = (int)std::ceil(dmax / dt_s) + 3;
+    const int r_min = (int)std::ceil(dmax / dt_s) + 3 + kMaxFuse;
     R = 1;
     while (R < r_min) R <<= 1;
 
@@ -444,6 +446,21 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
             CK(cudaMemsetAsync(D.post_t, 0, sizeof(double) * (size_t)kPostRing * p.n, st));
             CK(cudaMemsetAsync(D.post_n, 0, sizeof(uint32_t) * (size_t)p.n, st));
             CK(cudaMemsetAsync(D.post_flushed, 0, sizeof(uint32_t) * (size_t)p.n, st));
+            // one rule on every plastic input: decay factors of the spike intervals
+            int rule_one = -2;
+            for (int64_t i = p.first; i < p.first + p.n && rule_one != -1; ++i)
+                for (int64_t e = in_ptr[i]; e < plastic_end[i]; ++e) {
+                    const int r = rule[tord[e]];
+                    if (rule_one == -2) rule_one = r;
+                    else if (rule_one != r) { rule_one = -1; break; }
+                }
+            D.post_rule = rule_one >= 0 ? rule_one : -1;
+            if (D.post_rule >= 0) {
+                if ((rc = dalloc((void **)&D.post_f, sizeof(DecayPair) * (size_t)kPostRing * p.n))) return rc;
+                CK(cudaMemsetAsync(D.post_f, 0, sizeof(DecayPair) * (size_t)kPostRing * p.n, st));
+            }
+        } else {
+            D.post_rule = -1;
         }
         p.has_out = false;
         int64_t max_out = 0, in_from_inputs = 0;
@@ -481,6 +498,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
             dyn.push_back({p.dev.post_t, sizeof(double) * (size_t)kPostRing * p.n});
             dyn.push_back({p.dev.post_n, sizeof(uint32_t) * (size_t)p.n});
             dyn.push_back({p.dev.post_flushed, sizeof(uint32_t) * (size_t)p.n});
+            if (p.dev.post_f) dyn.push_back({p.dev.post_f, sizeof(DecayPair) * (size_t)kPostRing * p.n});
         }
     }
     for (int q = 0; q < std::max(4, (int)chain_pop.size() - 1); ++q) {
@@ -672,27 +690,50 @@ void eb_ctx::fork_join(std::vector<std::function<void(cudaStream_t)>> &work) {
     }
 }
 
-// Deferred post-synaptic STDP: apply every noted spike to the synapses (on the
-// context stream, profiled as kind 4).  Runs at least every kPostRing steps.
-void eb_ctx::enqueue_flush() {
+// Deferred post-synaptic STDP: apply the noted spikes to the synapses (on the
+// context stream, profiled as kind 4).  A partial flush (at least every kPostGraph
+// steps) only takes the neurons whose rings could overflow before the next one; a
+// full flush (before the host reads or writes weights, or the eager-STDP
+// persistent kernel runs) takes every neuron with a pending spike.
+void eb_ctx::enqueue_flush(bool full) {
     steps_since_flush = 0;
-    for (size_t q = 0; q < pops.size(); ++q) {
-        const auto &p = pops[q];
-        if (!p.dev.post_t) continue;
-        cudaEvent_t a = nullptr;
-        prof_stream = stream;
-        prof_begin(4, (int)q, &a);
-        enq_count += 2;
-        launch_flush_post(p.dev, net, std::max(1, p.post_chunks), 148 * 4, stream);
-        prof_end(4, (int)q, a);
-    }
+    for (size_t q = 0; q < pops.size(); ++q) enqueue_flush_pop((int)q, full, stream);
+}
+
+void eb_ctx::enqueue_flush_pop(int q, bool full, cudaStream_t s) {
+    const auto &p = pops[q];
+    if (!p.dev.post_t) return;
+    const uint32_t keep = full ? 0u : (uint32_t)(kPostRing - kPostGraph);
+    cudaEvent_t a = nullptr;
+    prof_stream = s;
+    prof_begin(4, q, &a);
+    enq_count += 2;
+    launch_flush_post(p.dev, net, std::max(1, p.post_chunks), keep, 148 * 4, s);
+    prof_end(4, q, a);
 }
 
 int eb_ctx::flush_post() {
     if (!lazy_post || !finalized) return EB_OK;
-    enqueue_flush();
+    enqueue_flush(true);
     CK(cudaGetLastError());
     return EB_OK;
+}
+
+// Captured graph of K steps (cached per K; see build_graph).
+eb_ctx::CachedGraph *eb_ctx::graph_for(int K) {
+    if (!graphs_valid) {
+        for (auto &g : graph_cache) cudaGraphExecDestroy(g.exec);
+        graph_cache.clear();
+        graphs_valid = true;
+    }
+    for (auto &g : graph_cache)
+        if (g.K == K) return &g;
+    if (graph_cache.size() >= 8) {
+        cudaGraphExecDestroy(graph_cache.front().exec);
+        graph_cache.erase(graph_cache.begin());
+    }
+    if (build_graph(K)) return nullptr;
+    return &graph_cache.back();
 }
 
 void eb_ctx::enqueue_step(int rel) {
@@ -711,7 +752,7 @@ void eb_ctx::enqueue_step(int rel) {
     };
     if (has_inputs) {
         auto f = timed(0, -1, [this, rel, inv_dt, fan_blocks](cudaStream_t s) {
-            launch_input_push(net, rel, inv_dt, fan_blocks, input_threads, s);
+            launch_input_push(net, rel, 1, inv_dt, fan_blocks, input_threads, s);
         });
         if (inputs_concurrent) phase.push_back(f);
         else f(stream);
@@ -721,7 +762,7 @@ void eb_ctx::enqueue_step(int rel) {
         // spikes fan out inside the update kernel (arrivals land at step k+1 or later)
         const double push_inv_dt = pops[q].has_out ? inv_dt : 0.0;
         phase.push_back(timed(1, (int)q, [this, q, rel, push_inv_dt](cudaStream_t s) {
-            launch_update(pops[q].dev, net, rel, push_inv_dt, s);
+            launch_update(pops[q].dev, net, rel, 1, push_inv_dt, s);
         }));
     }
     fork_join(phase);
@@ -802,6 +843,13 @@ int eb_ctx::setup_persistent() {
 // else a chain touches belongs to its own population (state, spike lists, the
 // target-major synapse records and the deferred post-synaptic rings), so the
 // chains need no other edge and the steps run exactly as in step order.
+//
+// A launch may run S consecutive steps of a chain (its neurons' state stays in
+// registers) when no step inside the window needs another step of the same
+// window: every lag into a model population (lo) and every slot-reuse lag (R -
+// hi), its own population's included, is at least S.  Input chains may feed a
+// window of the same index (lo < S): they are captured first and wait for nothing
+// of that window.
 void eb_ctx::plan_chains(const std::vector<int64_t> &out_ptr, const std::vector<uint32_t> &out_tgt,
                          const std::vector<uint16_t> &out_units) {
     chain_pop.clear();
@@ -824,19 +872,25 @@ void eb_ctx::plan_chains(const std::vector<int64_t> &out_ptr, const std::vector<
         }
     }
     chain_deps.assign(nc, {});
+    int fuse = kMaxFuse;
     for (int a = 0; a < nc; ++a)
         for (int b = 0; b < nc; ++b) {
             const size_t e = (size_t)a * nc + b;
-            if (a == b || umax[e] < 0) continue;
+            if (umax[e] < 0) continue;
             const bool from_inputs = chain_pop[a] < 0;
             // inputs of step j are the spikes of [t_{j-1}, t_j): one step earlier than a
             // neuron's spike at t_j, so one step less of lower bound
             const int lo = std::max(from_inputs ? 0 : 1,
                                     (int)std::floor((double)umin[e] * 0.0001 / dt_s) - (from_inputs ? 2 : 1));
             const int hi = (int)std::ceil((double)umax[e] * 0.0001 / dt_s) + 2;
+            if (!from_inputs) fuse = std::min(fuse, lo);
+            fuse = std::min(fuse, R - hi);
+            if (a == b) continue;
             chain_deps[b].push_back({a, lo});
             chain_deps[a].push_back({b, R - hi});
         }
+    chain_fuse = 1;
+    while (chain_fuse * 2 <= fuse) chain_fuse *= 2;
     chains_ok = nc >= 2 && nc <= 8;
     for (auto &p : pops)
         if (p.kind != KIND_INPUT && p.has_plastic_in && !p.dev.post_t) chains_ok = false;  // eager post phase
@@ -845,35 +899,44 @@ void eb_ctx::plan_chains(const std::vector<int64_t> &out_ptr, const std::vector<
             if (x.lag < 0 || (x.lag == 0 && chain_pop[x.other] >= 0)) chains_ok = false;
 }
 
-// K steps as per-population chains (see plan_chains), joined at the end.
+// K steps as per-population chains (see plan_chains), joined at the end; each
+// launch runs a window of S steps (S divides K).  A population's partial flush of
+// deferred post-synaptic STDP only touches its own synapses and rings, so it runs
+// in the population's chain every kPostGraph steps (and at the end of the graph).
 void eb_ctx::enqueue_chains(int K) {
     const int nc = (int)chain_pop.size();
-    while ((int)chain_ev.size() < nc * K) {
+    int S = chain_fuse;
+    while (K % S) S >>= 1;
+    const int W = K / S;
+    while ((int)chain_ev.size() < nc * W) {
         cudaEvent_t e;
         cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
         chain_ev.push_back(e);
     }
-    auto ev = [&](int c, int r) { return chain_ev[(size_t)c * K + r]; };
+    auto ev = [&](int c, int w) { return chain_ev[(size_t)c * W + w]; };
     auto strm = [&](int c) { return c == 0 ? stream : side[c - 1]; };
     const double inv_dt = 1.0 / dt_s;
     cudaEventRecord(fork_ev[0], stream);
     for (int c = 1; c < nc; ++c) cudaStreamWaitEvent(strm(c), fork_ev[0], 0);
-    for (int r = 0; r < K; ++r)
+    for (int w = 0; w < W; ++w)
         for (int c = 0; c < nc; ++c) {
             cudaStream_t s = strm(c);
             for (auto &d : chain_deps[c]) {
-                const int x = r - d.lag;
-                if (x >= 0) cudaStreamWaitEvent(s, ev(d.other, x), 0);
+                // the window's last step needs step x of the other chain
+                const int x = w * S + S - 1 - d.lag;
+                if (x >= 0) cudaStreamWaitEvent(s, ev(d.other, x / S), 0);
             }
             const int q = chain_pop[c];
             if (q < 0) {
-                launch_input_push(net, r, inv_dt, 148 * 4, input_threads, s);
+                launch_input_push(net, w * S, S, inv_dt, 148 * 4, input_threads, s);
             } else {
                 const double push_inv_dt = pops[q].has_out ? inv_dt : 0.0;
-                launch_update(pops[q].dev, net, r, push_inv_dt, s);
+                launch_update(pops[q].dev, net, w * S, S, push_inv_dt, s);
+                const int end = (w + 1) * S;
+                if (lazy_post && (end % kPostGraph == 0 || end == K)) enqueue_flush_pop(q, false, s);
             }
             enq_count++;
-            cudaEventRecord(ev(c, r), s);
+            cudaEventRecord(ev(c, w), s);
         }
     for (int c = 1; c < nc; ++c) {
         cudaEventRecord(join_ev[c], strm(c));
@@ -882,22 +945,27 @@ void eb_ctx::enqueue_chains(int K) {
 }
 
 int eb_ctx::build_graph(int K) {
-    if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+    const int since_flush = steps_since_flush;  // capturing flushes nothing yet
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     enq_count = 0;
-    if (chains_ok && chains_enabled) enqueue_chains(K);
-    else
-        for (int r = 0; r < K; ++r) enqueue_step(r);
-    if (lazy_post) enqueue_flush();
-    graph_kernels = enq_count + 1;
+    if (chains_ok && chains_enabled) {
+        enqueue_chains(K);
+    } else {
+        for (int r = 0; r < K; ++r) {
+            enqueue_step(r);
+            if (lazy_post && ((r + 1) % kPostGraph == 0 || r + 1 == K)) enqueue_flush(false);
+        }
+    }
+    const int kernels = enq_count + 1;
     launch_advance(d_step, K, stream);
     CK(cudaStreamEndCapture(stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&graph_exec, g, 0);
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) { set_error("cudaGraphInstantiate: %s", cudaGetErrorString(e)); return EB_ERR_CUDA; }
-    graph_K = K;
-    graphs_valid = true;
+    graph_cache.push_back({K, kernels, exec});
+    steps_since_flush = since_flush;
     return EB_OK;
 }
 
@@ -913,13 +981,13 @@ int eb_ctx::run_async(int64_t n) {
         trace_pending = false;
         graphs_valid = false;
     }
-    int K = graph_steps > 0 ? graph_steps : 64;
-    if (lazy_post && K > kPostRing) K = kPostRing;  // a graph's spikes must fit the rings
+    const int K = graph_steps > 0 ? graph_steps : kDefaultGraph;
     int64_t done = 0;
     if (persistent && persist_ok && !profile) {
+        if (lazy_post) enqueue_flush(true);  // the persistent kernel applies post-synaptic STDP eagerly
         if (pops_dirty) {
             // the persistent kernel applies post-synaptic STDP at each spike (its own
-            // phase); every run ends with a flush, so no deferred spike is pending here
+            // phase); the flush above left no deferred spike pending
             std::vector<PopDev> h;
             for (auto &p : pops)
                 if (p.kind != KIND_INPUT) {
@@ -927,6 +995,7 @@ int eb_ctx::run_async(int64_t n) {
                     h.back().post_t = nullptr;
                     h.back().post_n = nullptr;
                     h.back().post_flushed = nullptr;
+                    h.back().post_f = nullptr;
                 }
             CK(cudaMemcpyAsync(d_pops, h.data(), sizeof(PopDev) * h.size(), cudaMemcpyHostToDevice, stream));
             pops_dirty = false;
@@ -949,11 +1018,12 @@ int eb_ctx::run_async(int64_t n) {
         cudaGraphExec_t ge;
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         enq_count = 0;
+        if (lazy_post && steps_since_flush) enqueue_flush(false);
         for (int64_t r = 0; r < n; ++r) {
             enqueue_step((int)r);
-            if (lazy_post && (r + 1) % kPostRing == 0) enqueue_flush();
+            if (lazy_post && (r + 1) % kPostGraph == 0) enqueue_flush(false);
         }
-        if (lazy_post) enqueue_flush();
+        if (lazy_post) enqueue_flush(false);
         launch_advance(d_step, (int)n, stream);
         CK(cudaStreamEndCapture(stream, &g));
         CK(cudaGraphInstantiate(&ge, g, 0));
@@ -965,27 +1035,32 @@ int eb_ctx::run_async(int64_t n) {
         steps_done = k_end;
         return EB_OK;
     }
-    if (K > 1 && n >= K) {
-        if (!graphs_valid || graph_K != K)
-            if ((rc = build_graph(K))) return rc;
-        while (n - done >= K) {
-            CK(cudaGraphLaunch(graph_exec, stream));
-            launches += graph_kernels;
-            done += K;
+    // whole graphs of K steps, then one graph of the remainder when it is long
+    // enough to pay for its capture (cached, so repeated run lengths reuse it)
+    for (int pass = 0; pass < 2 && K > 1; ++pass) {
+        const int Kp = pass == 0 ? K : (int)(n - done);
+        if (n - done < Kp || Kp < kMinGraph) continue;
+        CachedGraph *g = graph_for(Kp);
+        if (!g) return EB_ERR_CUDA;
+        if (lazy_post && steps_since_flush) {  // a graph starts with every ring at most kPostRing - kPostGraph full
+            enq_count = 0;
+            enqueue_flush(false);
+            launches += enq_count;
         }
+        while (n - done >= Kp) {
+            CK(cudaGraphLaunch(g->exec, stream));
+            launches += g->kernels;
+            done += Kp;
+        }
+        steps_since_flush = 0;  // every graph ends with a partial flush
     }
     while (done < n) {
         enq_count = 0;
         enqueue_step(0);
         launch_advance(d_step, 1, stream);
-        if (lazy_post && ++steps_since_flush == kPostRing) enqueue_flush();
+        if (lazy_post && ++steps_since_flush == kPostGraph) enqueue_flush(false);
         launches += enq_count + 1;
         done++;
-    }
-    if (lazy_post && steps_since_flush) {
-        enq_count = 0;
-        enqueue_flush();
-        launches += enq_count;
     }
     CK(cudaGetLastError());
     steps_done = k_end;
@@ -1034,8 +1109,13 @@ int eb_ctx::snapshot(int slot) {
         CK(cudaMemcpyAsync((*bufs)[i], dyn[i].first, dyn[i].second, cudaMemcpyDeviceToDevice, stream));
     bool found = false;
     for (auto &h : snap_host)
-        if (h.slot == slot) { h.steps_done = steps_done; h.spikes_drained = spikes_drained; found = true; }
-    if (!found) snap_host.push_back({slot, steps_done, spikes_drained});
+        if (h.slot == slot) {
+            h.steps_done = steps_done;
+            h.spikes_drained = spikes_drained;
+            h.steps_since_flush = steps_since_flush;
+            found = true;
+        }
+    if (!found) snap_host.push_back({slot, steps_done, spikes_drained, steps_since_flush});
     CK(cudaStreamSynchronize(stream));
     return EB_OK;
 }
@@ -1048,14 +1128,17 @@ int eb_ctx::restore(int slot) {
     for (size_t i = 0; i < dyn.size(); ++i)
         CK(cudaMemcpyAsync(dyn[i].first, (*bufs)[i], dyn[i].second, cudaMemcpyDeviceToDevice, stream));
     for (auto &h : snap_host)
-        if (h.slot == slot) { steps_done = h.steps_done; }
+        if (h.slot == slot) {
+            steps_done = h.steps_done;
+            steps_since_flush = h.steps_since_flush;
+        }
     CK(cudaMemsetAsync(net.rec_count, 0, sizeof(unsigned long long), stream));
     CK(cudaStreamSynchronize(stream));
     return EB_OK;
 }
 
 eb_ctx::~eb_ctx() {
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto &g : graph_cache) cudaGraphExecDestroy(g.exec);
     for (auto s : side) cudaStreamDestroy(s);
     for (auto e : chain_ev) cudaEventDestroy(e);
     for (auto e : fork_ev) cudaEventDestroy(e);
@@ -1323,6 +1406,8 @@ int eb_get_trace(eb_ctx *ctx, float *out) {
 int eb_get_weights(eb_ctx *ctx, float *w) {
     if (!ctx || !w) { set_error("bad argument"); return EB_ERR_ARG; }
     if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
+    int rc;
+    if ((rc = ctx->flush_post())) return rc;  // deferred post-synaptic updates first
     CK(cudaStreamSynchronize(ctx->stream));
     const int64_t m = (int64_t)ctx->src.size();
     std::vector<SynRec> h(m);
@@ -1336,6 +1421,8 @@ int eb_set_weights(eb_ctx *ctx, const float *w) {
     if (!ctx->finalized) { set_error("not finalized"); return EB_ERR_STATE; }
     const int64_t m = (int64_t)ctx->src.size();
     std::vector<SynRec> h(m);
+    int rc;
+    if ((rc = ctx->flush_post())) return rc;  // pending post-synaptic updates belong to the old weights
     CK(cudaStreamSynchronize(ctx->stream));
     if (m) CK(cudaMemcpy(h.data(), ctx->net.syn, sizeof(SynRec) * (size_t)m, cudaMemcpyDeviceToHost));
     for (int64_t k = 0; k < m; ++k) h[ctx->tpos_of[k]].w = w[k];

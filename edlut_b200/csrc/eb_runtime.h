@@ -15,7 +15,8 @@ namespace eb {
 
 void set_error(const char *fmt, ...);
 
-
+// Most steps one launch of a captured graph runs for one population.
+constexpr int kMaxFuse = 8;
 
 struct HostPop {
     int kind = KIND_INPUT, integ = 0, bdf_order = 0;
@@ -80,6 +81,7 @@ struct eb_ctx {
     std::vector<std::vector<ChainDep>> chain_deps;
     std::vector<cudaEvent_t> chain_ev;         // [chain][step of the graph]
     bool chains_ok = false, chains_enabled = true;
+    int chain_fuse = 1;                        // steps per launch in a chain (a power of two)
     // time grid and inputs
     std::vector<double> t_host;
     double *d_tstep = nullptr;
@@ -99,15 +101,17 @@ struct eb_ctx {
     int64_t steps_done = 0;
     int64_t spikes_drained = 0;
     int graph_steps = 0;
-    cudaGraphExec_t graph_exec = nullptr;
-    int graph_K = 0;
+    struct CachedGraph { int K, kernels; cudaGraphExec_t exec; };
+    std::vector<CachedGraph> graph_cache;   // captured graphs by step count (at most 8)
+    static constexpr int kMinGraph = 8;     // shorter remainders run launch by launch
+    static constexpr int kDefaultGraph = 512;  // steps per captured graph
     bool graph_inputs = false;
     bool graphs_valid = false;
     bool trace_pending = false;
     size_t trace_bytes = 0;
     int64_t staged_until = 0;
     int64_t launches = 0;          // kernels launched (graph nodes counted per replay)
-    int enq_count = 0, graph_kernels = 0;      // input ranges valid for steps <= staged_until
+    int enq_count = 0;                      // kernels enqueued by the current capture or step
     // per-kernel profiling (plain launches with CUDA events around each kernel)
     bool profile = false;
     cudaStream_t prof_stream = nullptr;
@@ -122,7 +126,7 @@ struct eb_ctx {
     // dynamic device state (what a snapshot copies): (pointer, bytes)
     std::vector<std::pair<void *, size_t>> dyn;
     std::vector<std::pair<int, std::vector<void *>>> snapshots;
-    struct HostSnap { int slot; int64_t steps_done, spikes_drained; };
+    struct HostSnap { int slot; int64_t steps_done, spikes_drained; int steps_since_flush; };
     std::vector<HostSnap> snap_host;
 
     int dalloc(void **p, size_t bytes);
@@ -138,12 +142,14 @@ struct eb_ctx {
     void prof_end(int kind, int pop, cudaEvent_t a);
     int prof_collect();
     int build_graph(int K);
+    CachedGraph *graph_for(int K);
     void plan_chains(const std::vector<int64_t> &out_ptr, const std::vector<uint32_t> &out_tgt,
                      const std::vector<uint16_t> &out_units);
     void enqueue_chains(int K);
     int setup_persistent();
     int seed_generators();
-    void enqueue_flush();
+    void enqueue_flush(bool full);
+    void enqueue_flush_pop(int q, bool full, cudaStream_t s);
     int flush_post();
     bool lazy_post = false;       // some population defers post-synaptic STDP
     int steps_since_flush = 0;

@@ -8,7 +8,12 @@ enum Kind : int { KIND_INPUT = 0, KIND_LIF = 1, KIND_ADEX = 2, KIND_HH = 3, KIND
 enum Integ : int { INTEG_EULER = 0, INTEG_RK2 = 1, INTEG_RK4 = 2, INTEG_BDF = 3 };
 
 constexpr int kMaxVars = 8;
-constexpr int kPostRing = 64;  // spikes kept per neuron for deferred post-synaptic STDP
+// Deferred post-synaptic STDP: each neuron keeps its last kPostRing spike times.
+// A flush runs at least every kPostGraph steps and brings up to date every neuron
+// with more than kPostRing - kPostGraph spikes not yet applied to its synapses, so
+// no synapse ever has more than kPostRing of its target's spikes pending.
+constexpr int kPostRing = 128;
+constexpr int kPostGraph = 64;
 constexpr int kNmdaTable = 256;
 constexpr int kExptTable = 1024 * 16;
 constexpr int kHHTable = 1024 * 256;
@@ -28,6 +33,12 @@ struct alignas(16) Arrival {
     double a;
     uint32_t spos;
     uint32_t tpos;
+};
+
+// Trace decay factors of one interval (pre- and post-synaptic time constants).
+struct alignas(8) DecayPair {
+    float pre;
+    float post;
 };
 
 // One synapse in target-major order: everything a delivered spike and the two
@@ -76,11 +87,16 @@ struct PopDev {
     uint32_t *lcg;
     const double *pthr;
     // Deferred post-synaptic STDP: the times of each neuron's recent spikes,
-    // post_t[slot * n + i] with slot = spike number % kPostRing, and spike counts;
+    // post_t[i * kPostRing + slot] with slot = spike number % kPostRing, and spike counts;
     // null when the population applies post-synaptic STDP eagerly.
     double *post_t;
     uint32_t *post_n;
     uint32_t *post_flushed;  // post_n at the last flush
+    // The trace decay factors of the interval ending at each ring spike (from the
+    // spike before it), post_f[i * kPostRing + slot] = {pre, post}, for the population's one
+    // plastic rule post_rule; null (post_rule -1) when its plastic synapses mix rules.
+    DecayPair *post_f;
+    int post_rule;
 };
 
 // Network-wide device pointers, passed by value to the kernels.

@@ -198,6 +198,12 @@ class Simulation:
         check(self._L.eb_get_population_events(self._h, int(pop), ctypes.byref(e)))
         return e.value
 
+    def launch_count(self) -> int:
+        """Kernels launched so far (graph nodes counted per replay)."""
+        n = ctypes.c_int64(0)
+        check(self._L.eb_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
     def device_bytes(self) -> int:
         b = ctypes.c_int64(0)
         check(self._L.eb_device_bytes(self._h, ctypes.byref(b)))

@@ -113,9 +113,11 @@ int eb_load_input_file(eb_ctx *ctx, const char *input_file);
 
 /* ----------------------------------------------------------------- run --- */
 /* Advance n_steps integration steps (each: deliveries, neuron updates, spikes, STDP),
- * replaying captured CUDA graphs of `graph_steps` steps (0: default 64; 1: plain
- * launches).  Blocks until done.  Replaces the per-step TimeEventUpdateNeurons /
- * TimeDrivenInternalSpike / PropagatedSpikeGroup cycle. */
+ * replaying captured CUDA graphs of `graph_steps` steps (0: default 512; 1: plain
+ * launches; a shorter remainder of 8 steps or more gets a graph of its own).  In a
+ * graph each population is a chain of launches, each running up to 8 steps when
+ * the delays allow.  Blocks until done.  Replaces the per-step
+ * TimeEventUpdateNeurons / TimeDrivenInternalSpike / PropagatedSpikeGroup cycle. */
 int eb_run(eb_ctx *ctx, int64_t n_steps);
 int eb_set_graph_steps(eb_ctx *ctx, int graph_steps);
 /* on != 0: run all phases of up to 1000 steps in one cooperative persistent

@@ -92,3 +92,51 @@ def test_gpu_wide_fanin_matches_oracle(oracle, persistent):
     np.testing.assert_array_equal(r["trace"], o["trace"].astype(np.float32))
     np.testing.assert_array_equal(r["w"], o["w_final"].astype(np.float32))
     assert r["counters"]["events"] == o["n_events"]
+
+
+def test_gpu_fused_windows_equal_single_steps():
+    """With 1 ms delays at 0.1 ms steps a launch of the captured graph runs 8 steps
+    of a population: 128 steps of the small cerebellar case (one graph) take 3
+    chains x 16 windows + two deferred-STDP flushes of the Purkinje chain (2
+    launches each) + the step counter (1) launches; spikes, traces and weights
+    equal those of one launch per step."""
+    from edlut_b200.simulation import Simulation
+    net, t, c, _, trace = build_case("cereb_small_rk4")
+    out = []
+    for graph_steps in (0, 1):
+        sim = Simulation.from_description(net, graph_steps=graph_steps)
+        sim.inject_spikes(t, c)
+        sim.set_trace(trace[1], trace[2], 128)
+        l0 = sim.launch_count()
+        sim.run(128)
+        st, ce = sim.spikes()
+        out.append((spike_pairs(st, ce), sim.get_trace(), sim.weights(), sim.launch_count() - l0))
+        sim.close()
+    (s0, tr0, w0, n0), (s1, tr1, w1, _) = out
+    assert n0 == 3 * 16 + 2 * 2 + 1, n0
+    np.testing.assert_array_equal(s0, s1)
+    np.testing.assert_array_equal(tr0, tr1)
+    np.testing.assert_array_equal(w0, w1)
+
+
+@pytest.mark.parametrize("name", ["cereb_small_rk4", "adex_rk4_stdp"])
+def test_gpu_uneven_runs_match_fixture(name):
+    """Runs of uneven lengths mix whole graphs, remainder graphs and single-step
+    launches, with deferred post-synaptic STDP carried across them (partial flushes
+    between runs, a full one before the weights are read): the result is the
+    reference's."""
+    from edlut_b200.simulation import Simulation
+    net, t, c, nsteps, trace = build_case(name)
+    g = load_golden(name)
+    sim = Simulation.from_description(net)
+    sim.inject_spikes(t, c)
+    done = 0
+    for n in [100, 37, 5, 64, 200, 3, 129, 1, 70]:
+        sim.run(n)
+        done += n
+    sim.run(nsteps - done)
+    st, ce = sim.spikes()
+    np.testing.assert_array_equal(spike_pairs(st, ce), spike_pairs(g["spike_step"], g["spike_cell"]))
+    if "w_final" in g:
+        np.testing.assert_array_equal(sim.weights(), g["w_final"])
+    sim.close()
