@@ -134,10 +134,13 @@ def layer_starts(net):
     return [int(x) for x in np.cumsum([0] + [l.n for l in net.layers])]
 
 
-def roofline_bytes(net, pop_events, pop_spikes, n_int):
+def roofline_bytes(net, pop_events, pop_spikes, n_int, window=1):
     """Algorithmic bytes per launch of each profiled kernel, keyed like the profile
     ("update[granule]", ...), from the events delivered into each population and the
-    spikes of each population over `n_int` integration steps."""
+    spikes of each population over `n_int` integration steps, for launches that run
+    `window` steps: a neuron's state is read and written once per launch, events and
+    fan-out count for every step of the window.  The deferred post-synaptic flush
+    has no entry (the synapses it takes depend on the spike history)."""
     src = np.asarray(net.src)
     tgt = np.asarray(net.tgt)
     plastic = np.asarray(net.wchange) >= 0
@@ -150,12 +153,10 @@ def roofline_bytes(net, pop_events, pop_spikes, n_int):
             mdl = "AdEx" if "AdEx" in l.model else "HH" if "HH" in l.model else "LIF"
             unit = BYTES_PER_UNIT[mdl] + (96 if mdl == "HH" and l.integrator == "BDF" else 0)
             ev = pop_events[q] / n_int
-            out["update[%s]" % l.name] = unit * l.n + EVENT_BYTES * ev * (1.0 + frac_plastic)
+            out["update[%s]" % l.name] = unit * l.n + window * EVENT_BYTES * ev * (1.0 + frac_plastic)
             if frac_plastic > 0:
                 per_neuron = int((in_pop & plastic).sum()) / max(1, l.n)
                 out["post_stdp[%s]" % l.name] = EVENT_BYTES * per_neuron * pop_spikes[q] / n_int
-                # deferred form: one flush per 64 steps applies their post spikes
-                out["flush_post[%s]" % l.name] = 64 * out["post_stdp[%s]" % l.name]
         # fan-out launched from this population's spikes: 8 B per event it writes
         from_pop = (src >= starts[q]) & (src < starts[q + 1])
         if from_pop.any():
@@ -164,7 +165,7 @@ def roofline_bytes(net, pop_events, pop_spikes, n_int):
             # input spikes fan out in their own kernel; model neurons' spikes inside the
             # population's update kernel
             key = "input_push[-]" if l.model == "InputSpikeNeuronModel" else "update[%s]" % l.name
-            out[key] = out.get(key, 0.0) + EVENT_BYTES * ev_out / n_int
+            out[key] = out.get(key, 0.0) + window * EVENT_BYTES * ev_out / n_int
     return out
 
 
@@ -241,8 +242,8 @@ def run_ours(args):
     # per-kernel durations: the same steps replayed as a graph with event-record
     # nodes around every kernel on the stream it runs on
     _lib.check(L.eb_set_profile(sim._h, 1))
-    for _ in range(prof_steps * STEPS_PER_BENCH_STEP // 250):
-        sim.run(250)
+    for _ in range(prof_steps):
+        sim.run(STEPS_PER_BENCH_STEP)  # a multiple of 8: the run path's 8-step windows
     n = ctypes.c_int(0)
     cap = 64
     kinds = (ctypes.c_int * cap)()
@@ -282,20 +283,25 @@ def run_ours(args):
         d2h += len(st) * 8 + 8
     e2e_s = max_over_ranks(e2e_s, world)
 
-    # roofline: algorithmic bytes of each kernel per launch (neuron state 32 B per
-    # LIF/AdEx update, 48 B per HH update; 8 B per delivered event, +8 B when the
-    # synapse is plastic; post-synaptic STDP 8 B per plastic input synapse of each
-    # spiking neuron), divided by its measured average launch time
+    # roofline: algorithmic bytes of each kernel per launch -- a launch runs
+    # `window` steps of its population (neuron state read and written once per
+    # launch, BYTES_PER_UNIT per neuron; per delivered event 8 B, +8 B when the
+    # synapse is plastic, and 8 B per fanned-out event, every step) -- divided by
+    # its measured average launch time
     peak, peak_kind = measured_peaks()
     n_int = STEPS_PER_BENCH_STEP * K
-    alg = roofline_bytes(net, pop_events, pop_spikes, n_int)
-    for p in prof:
-        p["alg_bytes_per_launch"] = alg.get(p["kernel"], 0.0)
-        p["achieved_gbs"] = p["alg_bytes_per_launch"] / (p["avg_us"] * 1e-6) / 1e9
-    top = prof[0]
-    achieved = top["achieved_gbs"]
     n_prof_steps = prof_steps * STEPS_PER_BENCH_STEP
-    step_bytes = sum(alg.get(p["kernel"], 0.0) * p["launches"] for p in prof) / n_prof_steps
+    for p in prof:
+        window = max(1, round(n_prof_steps / max(1, p["launches"]))) if p["kernel"].startswith(("update", "input")) else 1
+        p["steps_per_launch"] = window
+        alg = roofline_bytes(net, pop_events, pop_spikes, n_int, window)
+        p["alg_bytes_per_launch"] = alg.get(p["kernel"])
+        p["achieved_gbs"] = (p["alg_bytes_per_launch"] / (p["avg_us"] * 1e-6) / 1e9
+                             if p["alg_bytes_per_launch"] is not None else None)
+    top = next(p for p in prof if p["alg_bytes_per_launch"] is not None)
+    achieved = top["achieved_gbs"]
+    step_bytes = sum(p["alg_bytes_per_launch"] * p["launches"] for p in prof
+                     if p["alg_bytes_per_launch"] is not None) / n_prof_steps
     step_gbs = step_bytes / (sec / n_int) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")
@@ -322,7 +328,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "kernel": top["kernel"], "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "alg_bytes_per_launch": top["alg_bytes_per_launch"],
-                     "avg_launch_us": top["avg_us"]},
+                     "avg_launch_us": top["avg_us"], "steps_per_launch": top["steps_per_launch"]},
         "step_roofline": {"alg_bytes_per_integration_step": step_bytes, "achieved": step_gbs,
                           "unit": "GB/s", "frac": step_gbs / peak},
         "kernels": prof[:8],

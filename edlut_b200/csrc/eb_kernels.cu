@@ -120,6 +120,7 @@ __device__ __forceinline__ void apply_pending(const NetDev &N, const Ring &ring,
     if (rule >= 0 && r.rule == rule) {
         const float a = N.rule_par[rule * 6];
         float w = r.w, pre = r.pre, post = r.post;
+#pragma unroll 4
         for (uint32_t q = lo + 1; q < c; ++q) {
             const DecayPair f = ring.fac(q % kPostRing);
             pre = pre * f.pre;
@@ -478,17 +479,47 @@ static_assert(kRankSort <= kWideThreads && kWideThreads == kNarrowTile, "wide bl
 
 struct WideSmem {
     int spiked;                         // the block's neuron spiked this step (fused fan-out)
+    int ring_ok;                        // ring, ring_f and ring_n hold the neuron's ring
     uint32_t ring_n;                    // post-synaptic spikes noted so far (deferred STDP)
+    uint32_t next_c;                    // next step's arrival count (copied ahead)
     float g[3];                         // conductances handed to the per-type adders
     unsigned long long khi[kRankSort];  // arrival time keys
     uint32_t klo[kRankSort];            // synapse order
     uint32_t rank[kRankSort];           // delivery position
     double ring[kPostRing];             // the neuron's deferred post-synaptic spike times
     DecayPair ring_f[kPostRing];           // and the decay factors of their intervals
+    Arrival next_rec[kRankSort];        // next step's first arrivals (copied ahead)
     Arrival sbuf[kWideSmem];
     float sw[kWideSmem];
     uint8_t sty[kWideSmem];
 };
+
+// Asynchronous global -> shared copies (cp.async): the block copies the next
+// step's arrivals while it works on this one; the copies complete at
+// cp_async_wait_all, before the next step's first barrier.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Copy step k's arrival count and its first n records (n <= the neuron's bucket
+// capacity) of neuron gi into S.next_c / S.next_rec.  Only for a step whose
+// bucket is final: a later step of the same launch (every delivery into it comes
+// from steps before the launch, or from input fan-out that precedes it).
+__device__ __forceinline__ void wide_prefetch(const NetDev &N, WideSmem &S, int64_t k, int64_t gi, int64_t rbase,
+                                              int n) {
+    const int slot = (int)(k & (N.R - 1));
+    const Arrival *r = N.rec + (int64_t)slot * N.cap_total + rbase;
+    for (int a = threadIdx.x; a < n; a += blockDim.x) cp_async16(&S.next_rec[a], r + a);
+    if (threadIdx.x == 0) cp_async4(&S.next_c, N.cnt + (int64_t)slot * N.n_neurons + gi);
+    cp_async_commit();
+}
 
 // Order-preserving integer key of an arrival time (-0 folded into +0).
 __device__ __forceinline__ unsigned long long time_key(double a) {
@@ -542,18 +573,32 @@ __device__ __forceinline__ void wide_fold(WideSmem &S, float *x, uint32_t c) {
 // One step of wide neuron i by the whole block; thread 0 holds its state in x and
 // ax (loaded and stored by the caller).
 template <int KIND, int INTEG>
+// pf_n: records of this step already copied to S.next_rec (with the count in
+// S.next_c; 0: none), updated for the next step when has_next (the next step is
+// in the same launch).
 __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
-                                          float *x, NeuronAux &ax, bool list, double push_inv_dt) {
+                                          float *x, NeuronAux &ax, bool list, double push_inv_dt, int &pf_n,
+                                          bool has_next) {
     constexpr int ND = Model<KIND>::ND;
     const int tid = threadIdx.x, nt = blockDim.x;
     const int slot = (int)(k & (N.R - 1));
     const int64_t gi = P.first + i;
-    __syncthreads();  // the block's previous neuron is done with S
+    if (pf_n > 0) cp_async_wait_all();
+    __syncthreads();  // the block's previous step is done with S; copied arrivals visible
     // every load that does not depend on another goes out first
     uint32_t *cp = N.cnt + (int64_t)slot * N.n_neurons + gi;
-    uint32_t c = *cp;
+    uint32_t c = pf_n > 0 ? S.next_c : *cp;
     const uint32_t capg = N.cap[gi];
     const int64_t rbase = N.cap_base[gi];
+    int next_n = 0;
+    // after a barrier that follows every thread's read of S.next_*: copy the next
+    // step's count and about as many records as this step had
+    auto issue_next = [&]() {
+        if (!has_next) return;
+        const uint32_t guess = ((c + c / 2 + 32) + 31) / 32 * 32;
+        next_n = (int)min(min(guess, capg), (uint32_t)kRankSort);
+        wide_prefetch(N, S, k + 1, gi, rbase, next_n);
+    };
     if (c) {
         if (c > capg) { if (tid == 0) atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
         Arrival *r = N.rec + (int64_t)slot * N.cap_total + rbase;
@@ -563,13 +608,13 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
             Arrival v;
             SynRec rec;
             if (own) {
-                v = r[tid];
+                v = tid < pf_n ? S.next_rec[tid] : r[tid];
                 if (!P.may_repeat) rec = N.syn[v.tpos];  // in flight while the positions are counted
                 S.khi[tid] = time_key(v.a);
                 S.klo[tid] = v.spos;
                 S.rank[tid] = 0;
             }
-            if (ring) {  // the neuron's deferred post-synaptic spikes (slots past the count are unused)
+            if (ring && !S.ring_ok) {  // the neuron's deferred post-synaptic spikes (slots past the count are unused)
                 for (int q = tid; q < kPostRing; q += nt) {
                     S.ring[q] = P.post_t[i * kPostRing + q];
                     if (P.post_f) S.ring_f[q] = P.post_f[i * kPostRing + q];
@@ -578,7 +623,11 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
             }
             if (tid == 32) prefetch_l1(N.rule_par);
             __syncthreads();
-            if (tid == 0) *cp = 0;
+            if (tid == 0) {
+                *cp = 0;
+                if (ring) S.ring_ok = 1;
+            }
+            issue_next();
             // position = arrivals before this one in (time, synapse order, bucket index)
             // order; per threads share each arrival's comparisons
             const int per = nt / (int)c;
@@ -625,6 +674,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
             }
             __syncthreads();
             if (tid == 0) *cp = 0;
+            issue_next();
             for (int size = 2; size <= n2; size <<= 1)
                 for (int stride = size >> 1; stride > 0; stride >>= 1) {
                     for (int a = tid; a < n2; a += nt) {
@@ -654,6 +704,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
             }
         } else {
             __syncthreads();  // every thread has read the count before it is cleared
+            issue_next();
             if (tid == 0) {
                 *cp = 0;
                 for (uint32_t a = 1; a < c; ++a) {  // rare: insertion sort in global memory
@@ -666,11 +717,22 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
             }
         }
         if (tid == 0) atomicAdd(P.events, (unsigned long long)c);
+    } else if (has_next) {
+        __syncthreads();  // every thread has read S.next_c
+        issue_next();
     }
     if (tid == 0) {
         const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax);
         S.spiked = sp ? 1 : 0;
-        if (sp && P.post_t) note_post_spike(P, N, i, k);
+        if (sp && P.post_t) {
+            note_post_spike(P, N, i, k);
+            if (S.ring_ok) {  // keep the staged ring current
+                const uint32_t n1 = P.post_n[i], q = (n1 - 1) % kPostRing;
+                S.ring_n = n1;
+                S.ring[q] = P.post_t[i * kPostRing + q];
+                if (P.post_f) S.ring_f[q] = P.post_f[i * kPostRing + q];
+            }
+        }
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
         if (sp) {
             if (list) {
@@ -688,6 +750,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
     }
     __syncthreads();
     if (push_inv_dt > 0.0 && S.spiked) push_from(P, N, k, gi, tid, blockDim.x, push_inv_dt);
+    pf_n = next_n;
 }
 
 template <int KIND, int INTEG>
@@ -698,8 +761,10 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
     if (threadIdx.x == 0) {
         load_state<KIND>(P, i, x);
         ax = load_aux<KIND, INTEG>(P, i);
+        S.ring_ok = 0;
     }
-    wide_step<KIND, INTEG>(P, N, k, i, S, x, ax, true, push_inv_dt);
+    int pf_n = 0;
+    wide_step<KIND, INTEG>(P, N, k, i, S, x, ax, true, push_inv_dt, pf_n, false);
     if (threadIdx.x == 0) {
         store_state<KIND>(P, i, x);
         store_aux<KIND, INTEG>(P, i, ax);
@@ -720,8 +785,11 @@ __global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N
         if (threadIdx.x == 0) {
             load_state<KIND>(P, i, x);
             ax = load_aux<KIND, INTEG>(P, i);
+            S.ring_ok = 0;
         }
-        for (int s = 0; s < nsteps; ++s) wide_step<KIND, INTEG>(P, N, k + s, i, S, x, ax, list, push_inv_dt);
+        int pf_n = 0;
+        for (int s = 0; s < nsteps; ++s)
+            wide_step<KIND, INTEG>(P, N, k + s, i, S, x, ax, list, push_inv_dt, pf_n, s + 1 < nsteps);
         if (threadIdx.x == 0) {
             store_state<KIND>(P, i, x);
             store_aux<KIND, INTEG>(P, i, ax);
@@ -1126,38 +1194,40 @@ void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks,
 // Bring every plastic synapse onto the population up to date with its target's
 // deferred post-synaptic spikes: items are (neuron, chunk of kPostThreads plastic
 // synapses), neurons without spikes since the last flush skipped.
-// Only neurons with more than keep pending spikes are brought up to date.  Items
-// are (neuron, chunk of kPostThreads plastic synapses); each block takes a
-// contiguous run of them, so it reads a neuron's count once and stages its ring in
-// shared memory once for all the chunks it takes of it.
-__global__ void __launch_bounds__(kPostThreads) k_flush_post(PopDev P, NetDev N, int max_chunks, uint32_t keep) {
+// Deferred post-synaptic flush in three launches: k_flush_select lists the neurons
+// with more than keep pending spikes (P.flush_list, count P.flush_list[P.n]);
+// k_flush_post brings their plastic synapses up to date, items (listed neuron,
+// chunk of kPostThreads synapses) in contiguous runs per block, so a block reads a
+// neuron's count and stages its ring in shared memory once for all its chunks;
+// k_flush_mark records the listed neurons as flushed and clears the list.
+__global__ void __launch_bounds__(256) k_flush_select(PopDev P, uint32_t keep) {
+    uint32_t *list = P.flush_list, *count = P.flush_list + P.n;
+    for (int64_t i = threadIdx.x; i < P.n; i += blockDim.x)
+        if (P.post_n[i] - P.post_flushed[i] > keep) list[atomicAdd(count, 1u)] = (uint32_t)i;
+}
+
+__global__ void __launch_bounds__(kPostThreads) k_flush_post(PopDev P, NetDev N, int max_chunks) {
     __shared__ double ring[kPostRing];
     __shared__ DecayPair fac[kPostRing];
     __shared__ uint32_t s_c;
-    __shared__ int s_go;
-    const int64_t items = P.n * (int64_t)max_chunks;
+    const int64_t items = (int64_t)P.flush_list[P.n] * max_chunks;
     const int64_t per = (items + gridDim.x - 1) / gridDim.x;
     const int64_t it0 = (int64_t)blockIdx.x * per, it1 = min(items, it0 + per);
     const int rule = P.post_f ? P.post_rule : -1;
     int64_t cur = -1;
     for (int64_t item = it0; item < it1; ++item) {
-        const int64_t i = item / max_chunks, ch = item % max_chunks;
-        if (i != cur) {
+        const int64_t li = item / max_chunks, ch = item - li * max_chunks;
+        const int64_t i = P.flush_list[li];
+        if (li != cur) {
             __syncthreads();  // the block is done with the previous neuron's ring
-            if (threadIdx.x == 0) {
-                s_c = P.post_n[i];
-                s_go = s_c - P.post_flushed[i] > keep;
+            if (threadIdx.x == 0) s_c = P.post_n[i];
+            for (int q = threadIdx.x; q < kPostRing; q += blockDim.x) {
+                ring[q] = P.post_t[i * kPostRing + q];
+                if (P.post_f) fac[q] = P.post_f[i * kPostRing + q];
             }
             __syncthreads();
-            if (s_go)
-                for (int q = threadIdx.x; q < kPostRing; q += blockDim.x) {
-                    ring[q] = P.post_t[i * kPostRing + q];
-                    if (P.post_f) fac[q] = P.post_f[i * kPostRing + q];
-                }
-            __syncthreads();
-            cur = i;
+            cur = li;
         }
-        if (!s_go) continue;
         const int64_t t = P.first + i;
         const int64_t tp = N.in_ptr[t] + ch * kPostThreads + threadIdx.x;
         if (tp >= N.plastic_end[t]) continue;
@@ -1171,14 +1241,21 @@ __global__ void __launch_bounds__(kPostThreads) k_flush_post(PopDev P, NetDev N,
     }
 }
 
-__global__ void k_flush_mark(PopDev P, uint32_t keep) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < P.n; i += (int64_t)gridDim.x * blockDim.x)
-        if (P.post_n[i] - P.post_flushed[i] > keep) P.post_flushed[i] = P.post_n[i];
+__global__ void __launch_bounds__(256) k_flush_mark(PopDev P) {
+    uint32_t *list = P.flush_list, *count = P.flush_list + P.n;
+    const uint32_t n = *count;
+    for (uint32_t a = threadIdx.x; a < n; a += blockDim.x) {
+        const uint32_t i = list[a];
+        P.post_flushed[i] = P.post_n[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *count = 0;
 }
 
 void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, uint32_t keep, int blocks, cudaStream_t st) {
-    k_flush_post<<<blocks, kPostThreads, 0, st>>>(P, N, max_chunks, keep);
-    k_flush_mark<<<(unsigned)std::min<int64_t>((P.n + 255) / 256, 1184), 256, 0, st>>>(P, keep);
+    k_flush_select<<<1, 256, 0, st>>>(P, keep);
+    k_flush_post<<<blocks, kPostThreads, 0, st>>>(P, N, max_chunks);
+    k_flush_mark<<<1, 256, 0, st>>>(P);
 }
 
 void launch_advance(int64_t *step, int K, cudaStream_t st) { k_advance<<<1, 1, 0, st>>>(step, K); }

@@ -14,7 +14,7 @@ void launch_push(const PopDev &P, const NetDev &N, int rel, double inv_dt, int b
 void launch_input_push(const NetDev &N, int rel, int nsteps, double inv_dt, int blocks, int threads, cudaStream_t st);
 void launch_post_stdp(const PopDev &P, const NetDev &N, int rel, int max_chunks, int blocks, cudaStream_t st);
 // Deferred post-synaptic STDP: apply the spikes noted since the last flush to the
-// synapses of every neuron with more than keep of them (2 launches).
+// synapses of every neuron with more than keep of them (3 launches).
 void launch_flush_post(const PopDev &P, const NetDev &N, int max_chunks, uint32_t keep, int blocks, cudaStream_t st);
 void launch_advance(int64_t *step, int K, cudaStream_t st);
 

@@ -446,6 +446,8 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
             CK(cudaMemsetAsync(D.post_t, 0, sizeof(double) * (size_t)kPostRing * p.n, st));
             CK(cudaMemsetAsync(D.post_n, 0, sizeof(uint32_t) * (size_t)p.n, st));
             CK(cudaMemsetAsync(D.post_flushed, 0, sizeof(uint32_t) * (size_t)p.n, st));
+            if ((rc = dalloc((void **)&D.flush_list, sizeof(uint32_t) * (size_t)(p.n + 1)))) return rc;
+            CK(cudaMemsetAsync(D.flush_list, 0, sizeof(uint32_t) * (size_t)(p.n + 1), st));
             // one rule on every plastic input: decay factors of the spike intervals
             int rule_one = -2;
             for (int64_t i = p.first; i < p.first + p.n && rule_one != -1; ++i)
@@ -707,8 +709,8 @@ void eb_ctx::enqueue_flush_pop(int q, bool full, cudaStream_t s) {
     cudaEvent_t a = nullptr;
     prof_stream = s;
     prof_begin(4, q, &a);
-    enq_count += 2;
-    launch_flush_post(p.dev, net, std::max(1, p.post_chunks), keep, 148 * 4, s);
+    enq_count += 3;
+    launch_flush_post(p.dev, net, std::max(1, p.post_chunks), keep, 148 * 8, s);
     prof_end(4, q, a);
 }
 
@@ -927,15 +929,19 @@ void eb_ctx::enqueue_chains(int K) {
                 if (x >= 0) cudaStreamWaitEvent(s, ev(d.other, x / S), 0);
             }
             const int q = chain_pop[c];
+            cudaEvent_t a = nullptr;
+            prof_stream = s;
+            prof_begin(q < 0 ? 0 : 1, q, &a);
             if (q < 0) {
                 launch_input_push(net, w * S, S, inv_dt, 148 * 4, input_threads, s);
             } else {
                 const double push_inv_dt = pops[q].has_out ? inv_dt : 0.0;
                 launch_update(pops[q].dev, net, w * S, S, push_inv_dt, s);
-                const int end = (w + 1) * S;
-                if (lazy_post && (end % kPostGraph == 0 || end == K)) enqueue_flush_pop(q, false, s);
             }
+            prof_end(q < 0 ? 0 : 1, q, a);
             enq_count++;
+            const int end = (w + 1) * S;
+            if (q >= 0 && lazy_post && (end % kPostGraph == 0 || end == K)) enqueue_flush_pop(q, false, s);
             cudaEventRecord(ev(c, w), s);
         }
     for (int c = 1; c < nc; ++c) {
@@ -1019,11 +1025,15 @@ int eb_ctx::run_async(int64_t n) {
         CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         enq_count = 0;
         if (lazy_post && steps_since_flush) enqueue_flush(false);
-        for (int64_t r = 0; r < n; ++r) {
-            enqueue_step((int)r);
-            if (lazy_post && (r + 1) % kPostGraph == 0) enqueue_flush(false);
+        if (chains_ok && chains_enabled && n <= (1 << 20)) {
+            enqueue_chains((int)n);  // the graph path's launches, each bracketed by events
+        } else {
+            for (int64_t r = 0; r < n; ++r) {
+                enqueue_step((int)r);
+                if (lazy_post && (r + 1) % kPostGraph == 0) enqueue_flush(false);
+            }
+            if (lazy_post) enqueue_flush(false);
         }
-        if (lazy_post) enqueue_flush(false);
         launch_advance(d_step, (int)n, stream);
         CK(cudaStreamEndCapture(stream, &g));
         CK(cudaGraphInstantiate(&ge, g, 0));

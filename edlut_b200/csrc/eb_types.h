@@ -97,6 +97,7 @@ struct PopDev {
     // plastic rule post_rule; null (post_rule -1) when its plastic synapses mix rules.
     DecayPair *post_f;
     int post_rule;
+    uint32_t *flush_list;  // [n + 1]: neurons a flush takes, their count last (zero between flushes)
 };
 
 // Network-wide device pointers, passed by value to the kernels.

@@ -181,10 +181,13 @@ int eb_stream(eb_ctx *ctx, void **stream);
 /* Move the input spikes and step tables of the next n_steps to the device now, so
  * a following eb_run of those steps does no host-to-device copy. */
 int eb_prestage(eb_ctx *ctx, int64_t n_steps);
-/* Per-kernel timing: with on != 0, runs use plain launches with CUDA events around
- * every kernel; eb_get_profile returns, per (kernel kind, population), the launch
- * count and total milliseconds.  kind: 0 input fan-out, 1 neuron update,
- * 2 post-synaptic STDP, 3 spike fan-out; pop: population index (-1: none). */
+/* Per-kernel timing: with on != 0, each run is one captured graph of its steps, the
+ * same launches as the run path (per-population chains, several steps per launch
+ * where the delays allow), with CUDA event records around every kernel on the
+ * stream it runs on; eb_get_profile returns, per (kernel kind, population), the
+ * launch count and total milliseconds.  kind: 0 input fan-out, 1 neuron update,
+ * 2 post-synaptic STDP, 3 spike fan-out, 4 deferred post-synaptic STDP flush;
+ * pop: population index (-1: none). */
 int eb_set_profile(eb_ctx *ctx, int on);
 int eb_get_profile(eb_ctx *ctx, int cap, int *n, int *kind, int *pop, int64_t *launches, double *total_ms);
 /* Number of library kernels launched so far (nodes of a replayed graph counted per replay). */

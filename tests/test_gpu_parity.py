@@ -97,7 +97,7 @@ def test_gpu_wide_fanin_matches_oracle(oracle, persistent):
 def test_gpu_fused_windows_equal_single_steps():
     """With 1 ms delays at 0.1 ms steps a launch of the captured graph runs 8 steps
     of a population: 128 steps of the small cerebellar case (one graph) take 3
-    chains x 16 windows + two deferred-STDP flushes of the Purkinje chain (2
+    chains x 16 windows + two deferred-STDP flushes of the Purkinje chain (3
     launches each) + the step counter (1) launches; spikes, traces and weights
     equal those of one launch per step."""
     from edlut_b200.simulation import Simulation
@@ -113,7 +113,7 @@ def test_gpu_fused_windows_equal_single_steps():
         out.append((spike_pairs(st, ce), sim.get_trace(), sim.weights(), sim.launch_count() - l0))
         sim.close()
     (s0, tr0, w0, n0), (s1, tr1, w1, _) = out
-    assert n0 == 3 * 16 + 2 * 2 + 1, n0
+    assert n0 == 3 * 16 + 2 * 3 + 1, n0
     np.testing.assert_array_equal(s0, s1)
     np.testing.assert_array_equal(tr0, tr1)
     np.testing.assert_array_equal(w0, w1)
