@@ -138,9 +138,13 @@ def roofline_bytes(net, pop_events, pop_spikes, n_int, window=1):
     """Algorithmic bytes per launch of each profiled kernel, keyed like the profile
     ("update[granule]", ...), from the events delivered into each population and the
     spikes of each population over `n_int` integration steps, for launches that run
-    `window` steps: a neuron's state is read and written once per launch, events and
-    fan-out count for every step of the window.  The deferred post-synaptic flush
-    has no entry (the synapses it takes depend on the spike history)."""
+    `window` steps.  Every unit counts for every step of the window: BYTES_PER_UNIT
+    per neuron-update (the state read and written once per step, although a launch
+    keeps it in registers between its steps), 8 B per delivered event (+8 B when the
+    synapse is plastic) and 8 B per fanned-out event.  "post_stdp[...]" is the
+    post-synaptic STDP of a population per integration step (8 B per plastic input
+    synapse per spike); it runs deferred, inside the update and the flush kernels,
+    so it counts only in the whole step's figure."""
     src = np.asarray(net.src)
     tgt = np.asarray(net.tgt)
     plastic = np.asarray(net.wchange) >= 0
@@ -153,7 +157,7 @@ def roofline_bytes(net, pop_events, pop_spikes, n_int, window=1):
             mdl = "AdEx" if "AdEx" in l.model else "HH" if "HH" in l.model else "LIF"
             unit = BYTES_PER_UNIT[mdl] + (96 if mdl == "HH" and l.integrator == "BDF" else 0)
             ev = pop_events[q] / n_int
-            out["update[%s]" % l.name] = unit * l.n + window * EVENT_BYTES * ev * (1.0 + frac_plastic)
+            out["update[%s]" % l.name] = window * (unit * l.n + EVENT_BYTES * ev * (1.0 + frac_plastic))
             if frac_plastic > 0:
                 per_neuron = int((in_pop & plastic).sum()) / max(1, l.n)
                 out["post_stdp[%s]" % l.name] = EVENT_BYTES * per_neuron * pop_spikes[q] / n_int
@@ -302,6 +306,8 @@ def run_ours(args):
     achieved = top["achieved_gbs"]
     step_bytes = sum(p["alg_bytes_per_launch"] * p["launches"] for p in prof
                      if p["alg_bytes_per_launch"] is not None) / n_prof_steps
+    step_bytes += sum(v for k, v in roofline_bytes(net, pop_events, pop_spikes, n_int).items()
+                      if k.startswith("post_stdp"))
     step_gbs = step_bytes / (sec / n_int) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "traffic.json")

@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OUT = os.path.join(OUT_DIR, "libedlut_b200.so")
-SOURCES = ["eb_kernels.cu", "eb_runtime.cu", "eb_fold.cu", "eb_sweep.cu", "eb_adjoint.cu", "eb_tables.cpp", "eb_cfg.cpp"]
+SOURCES = ["eb_kernels.cu", "eb_runtime.cu", "eb_record.cu", "eb_fold.cu", "eb_sweep.cu", "eb_adjoint.cu", "eb_tables.cpp", "eb_cfg.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

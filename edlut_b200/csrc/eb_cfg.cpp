@@ -158,6 +158,7 @@ extern "C" int eb_load_network_files(eb_ctx *ctx, const char *network_file, cons
             if ((rc = ctx->add_population(kind, nn, integ, order, dt, params.data(), (int)params.size(), nullptr)))
                 return rc;
         }
+        ctx->pops.back().output = outn != 0;
     }
     f.skip_comments();
     int nrules = 0;

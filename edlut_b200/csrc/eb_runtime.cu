@@ -14,6 +14,7 @@
 
 #include "edlut_b200.h"
 #include "eb_kernels.h"
+#include "eb_record.h"
 #include "eb_runtime.h"
 #include "eb_tables.h"
 
@@ -60,6 +61,15 @@ int eb_ctx::dalloc(void **p, size_t bytes) {
     allocs.push_back(*p);
     dev_bytes += (int64_t)bytes;
     return EB_OK;
+}
+
+void eb_ctx::dfree(void *p) {
+    for (size_t i = 0; i < allocs.size(); ++i)
+        if (allocs[i] == p) {
+            allocs.erase(allocs.begin() + (long)i);
+            cudaFree(p);
+            return;
+        }
 }
 
 void eb_ctx::dfree_all() {
@@ -1143,6 +1153,7 @@ int eb_ctx::restore(int slot) {
             steps_since_flush = h.steps_since_flush;
         }
     CK(cudaMemsetAsync(net.rec_count, 0, sizeof(unsigned long long), stream));
+    rec_step_lo = steps_done;
     CK(cudaStreamSynchronize(stream));
     return EB_OK;
 }
@@ -1156,6 +1167,7 @@ eb_ctx::~eb_ctx() {
     for (auto &r : prof_pending) { ev_pool.push_back(r.a); ev_pool.push_back(r.b); }
     for (auto e : ev_pool) cudaEventDestroy(e);
     dfree_all();
+    if (rec_host) cudaFreeHost(rec_host);
     if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -1335,14 +1347,44 @@ int eb_get_spikes(eb_ctx *ctx, int64_t cap, int64_t *n, int64_t *step, int64_t *
     int64_t have = (int64_t)std::min<unsigned long long>(cnt, (unsigned long long)ctx->rec_cap);
     *n = have;
     if (have > cap) { set_error("eb_get_spikes: %lld spikes, buffer holds %lld", (long long)have, (long long)cap); return EB_ERR_OVERFLOW; }
-    std::vector<unsigned long long> h(have);
-    if (have) CK(cudaMemcpy(h.data(), ctx->net.rec_buf, sizeof(unsigned long long) * (size_t)have, cudaMemcpyDeviceToHost));
-    std::sort(h.begin(), h.end());
+    if (have > ((int64_t)1 << 31)) { set_error("eb_get_spikes: more than 2^31 recorded spikes"); return EB_ERR_OVERFLOW; }
+    // sort on the device (eb_record.cu), copy through a pinned buffer, unpack
+    // while checking the order and the ranges
+    const int64_t s_lo = ctx->rec_step_lo, s_hi = ctx->steps_done;
+    if (have > 0) {
+        int rc;
+        if (have > ctx->rec_sort_cap) {
+            const int64_t ncap = std::max<int64_t>(have + have / 2, 1 << 16);
+            if (ctx->rec_tmp) { ctx->dfree(ctx->rec_tmp); ctx->rec_tmp = nullptr; }
+            if (ctx->rec_hist) { ctx->dfree(ctx->rec_hist); ctx->rec_hist = nullptr; }
+            if (ctx->rec_host) { cudaFreeHost(ctx->rec_host); ctx->rec_host = nullptr; }
+            ctx->rec_sort_cap = 0;
+            if ((rc = ctx->dalloc((void **)&ctx->rec_tmp, sizeof(unsigned long long) * (size_t)ncap))) return rc;
+            if ((rc = ctx->dalloc((void **)&ctx->rec_hist, sizeof(uint32_t) * eb::record_sort_hist_words(ncap)))) return rc;
+            CK(cudaHostAlloc((void **)&ctx->rec_host, sizeof(unsigned long long) * (size_t)ncap, cudaHostAllocDefault));
+            ctx->rec_sort_cap = ncap;
+        }
+        unsigned long long *sorted = nullptr;
+        CK(eb::sort_record(ctx->net.rec_buf, ctx->rec_tmp, ctx->rec_hist, have, s_lo, s_hi, ctx->n_neurons, ctx->stream,
+                           &sorted));
+        ctx->launches += eb::record_sort_launches(have, s_lo, s_hi, ctx->n_neurons);
+        CK(cudaMemcpyAsync(ctx->rec_host, sorted, sizeof(unsigned long long) * (size_t)have, cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    const unsigned long long *h = ctx->rec_host;
     for (int64_t i = 0; i < have; ++i) {
-        if (step) step[i] = (int64_t)(h[i] >> 32);
-        if (cell) cell[i] = (int64_t)(h[i] & 0xffffffffull);
+        const int64_t k = (int64_t)(h[i] >> 32), c = (int64_t)(h[i] & 0xffffffffull);
+        if ((i > 0 && h[i] <= h[i - 1]) || k <= s_lo || k > s_hi || c >= ctx->n_neurons) {
+            set_error("eb_get_spikes: spike record %lld (step %lld, neuron %lld) out of order or range", (long long)i,
+                      (long long)k, (long long)c);
+            return EB_ERR_STATE;
+        }
+        if (step) step[i] = k;
+        if (cell) cell[i] = c;
     }
     ctx->spikes_drained += have;
+    ctx->rec_step_lo = s_hi;
     CK(cudaMemset(ctx->net.rec_count, 0, sizeof(unsigned long long)));
     return EB_OK;
 }
@@ -1472,6 +1514,61 @@ int eb_set_poisson_rates(eb_ctx *ctx, int64_t first, int64_t n, const float *rat
                           cudaMemcpyHostToDevice));
         }
     }
+    return EB_OK;
+}
+
+int eb_set_output(eb_ctx *ctx, int pop, int on) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (pop < 0 || pop >= (int)ctx->pops.size()) { set_error("population %d out of range", pop); return EB_ERR_ARG; }
+    ctx->pops[pop].output = on != 0;
+    return EB_OK;
+}
+
+// FileOutputSpikeDriver::WriteSpike (src/communication/FileOutputSpikeDriver.cpp:
+// 40-46): one "%f\t%li" line per spike, the update time of its step and the
+// neuron, for the neurons of populations with the output flag.
+int eb_write_spikes(eb_ctx *ctx, const char *path, int append) {
+    if (!ctx || !path) { set_error("bad argument"); return EB_ERR_ARG; }
+    int64_t n = 0;
+    int rc = eb_get_spikes(ctx, 0, &n, nullptr, nullptr);
+    if (rc && rc != EB_ERR_OVERFLOW) return rc;
+    std::vector<int64_t> st(n), ce(n);
+    if (n && (rc = eb_get_spikes(ctx, n, &n, st.data(), ce.data()))) return rc;
+    FILE *f = std::fopen(path, append ? "a" : "w");
+    if (!f) { set_error("cannot open %s for writing", path); return EB_ERR_ARG; }
+    for (int64_t i = 0; i < n; ++i) {
+        if (!ctx->pops[ctx->pop_of[ce[i]]].output) continue;
+        double t;
+        eb_step_time(ctx, st[i], &t);
+        if (std::fprintf(f, "%f\t%li\n", t, (long)ce[i]) < 0) {
+            std::fclose(f);
+            set_error("write to %s failed", path);
+            return EB_ERR_ARG;
+        }
+    }
+    if (std::fclose(f) != 0) { set_error("write to %s failed", path); return EB_ERR_ARG; }
+    return EB_OK;
+}
+
+// Network::SaveWeights (src/spike/Network.cpp:1165-1202): the weights in
+// network-file order as runs of equal values, one "%i %g" line per run.
+int eb_save_weights(eb_ctx *ctx, const char *path) {
+    if (!ctx || !path) { set_error("bad argument"); return EB_ERR_ARG; }
+    const int64_t m = (int64_t)ctx->src.size();
+    std::vector<float> w(m);
+    int rc;
+    if (m && (rc = eb_get_weights(ctx, w.data()))) return rc;
+    FILE *f = std::fopen(path, "wt");
+    if (!f) { set_error("cannot open %s for writing", path); return EB_ERR_ARG; }
+    bool ok = true;
+    for (int64_t i = 0; i < m && ok;) {
+        const float v = w[i];
+        int64_t j = i + 1;
+        while (j < m && w[j] == v) ++j;
+        ok = std::fprintf(f, "%i %g\n", (int)(j - i), (double)v) > 0;
+        i = j;
+    }
+    if (std::fclose(f) != 0 || !ok) { set_error("write to %s failed", path); return EB_ERR_ARG; }
     return EB_OK;
 }
 

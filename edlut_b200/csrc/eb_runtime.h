@@ -25,6 +25,7 @@ struct HostPop {
     std::vector<float> params;
     int en = 0;                 // enabled conductance types (from the synapse types targeting it)
     bool has_out = false, has_plastic_in = false;
+    bool output = true;         // spikes go to eb_write_spikes (the layer line's output column)
     int post_chunks = 1;
     int push_threads = 32;
     std::vector<float> rates;   // Poisson generators: per-neuron frequency (Hz)
@@ -100,6 +101,12 @@ struct eb_ctx {
     // run state
     int64_t steps_done = 0;
     int64_t spikes_drained = 0;
+    // spike record drain: every recorded step is above rec_step_lo; device sort
+    // workspace and the pinned buffer the sorted records are copied through
+    int64_t rec_step_lo = 0;
+    unsigned long long *rec_tmp = nullptr, *rec_host = nullptr;
+    uint32_t *rec_hist = nullptr;
+    int64_t rec_sort_cap = 0;
     int graph_steps = 0;
     struct CachedGraph { int K, kernels; cudaGraphExec_t exec; };
     std::vector<CachedGraph> graph_cache;   // captured graphs by step count (at most 8)
@@ -130,6 +137,7 @@ struct eb_ctx {
     std::vector<HostSnap> snap_host;
 
     int dalloc(void **p, size_t bytes);
+    void dfree(void *p);
     void dfree_all();
     int add_population(int kind, int64_t n, int integ, int bdf_order, float dt, const float *params, int n_params,
                        int64_t *out_first);

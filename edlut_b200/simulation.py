@@ -9,6 +9,7 @@ read spikes, states and weights back.
 from __future__ import annotations
 
 import ctypes
+import os
 from typing import Optional, Sequence
 
 import numpy as np
@@ -182,6 +183,17 @@ class Simulation:
         w = np.zeros(max(self.n_synapses, 1), np.float32)
         check(self._L.eb_get_weights(self._h, _ptr(w, c_f32p)))
         return w[:self.n_synapses]
+
+    def write_spikes(self, path: str, append: bool = False) -> None:
+        """Drain recorded spikes into `path` in the reference's -of file format."""
+        check(self._L.eb_write_spikes(self._h, os.fsencode(path), int(bool(append))))
+
+    def set_output(self, pop: int, on: bool = True) -> None:
+        check(self._L.eb_set_output(self._h, int(pop), int(bool(on))))
+
+    def save_weights(self, path: str) -> None:
+        """Write the weights in the reference's weights-file format (-sf)."""
+        check(self._L.eb_save_weights(self._h, os.fsencode(path)))
 
     def set_weights(self, w) -> None:
         w = np.ascontiguousarray(w, np.float32)

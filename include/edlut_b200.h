@@ -146,6 +146,21 @@ int eb_set_record_capacity(eb_ctx *ctx, int64_t cap);
  * (src/communication/ArrayOutputSpikeDriver.cpp:56-80).  With cap too small, returns
  * EB_ERR_OVERFLOW and *n the required size without draining. */
 int eb_get_spikes(eb_ctx *ctx, int64_t cap, int64_t *n, int64_t *step, int64_t *cell);
+/* Drain recorded spikes (as eb_get_spikes) into a text file in the reference's
+ * output format, FileOutputSpikeDriver::WriteSpike
+ * (src/communication/FileOutputSpikeDriver.cpp:40-46, the -of option): one
+ * "%f\t%li" line per spike with the update time of its step and the neuron,
+ * sorted by (step, neuron), for the populations whose output flag is set (the
+ * output column of the network file's layer line; eb_add_population: set).
+ * append != 0 appends to the file.  Spikes of input neurons, which the caller
+ * supplied, are not recorded and not written. */
+int eb_write_spikes(eb_ctx *ctx, const char *path, int append);
+/* Output flag of population `pop` (eb_add_population order). */
+int eb_set_output(eb_ctx *ctx, int pop, int on);
+/* Write the weights in network-file order in the reference's weights-file format,
+ * Network::SaveWeights (src/spike/Network.cpp:1165-1202, the -sf option): runs of
+ * equal weights as "%i %g" lines.  The file loads back with eb_load_network_files. */
+int eb_save_weights(eb_ctx *ctx, const char *path);
 /* Update time of step k (double seconds, accumulated like the reference). */
 int eb_step_time(eb_ctx *ctx, int64_t k, double *t);
 /* State variable `var` (model order: V first, then the other differential variables,

@@ -140,7 +140,8 @@ def run_reference(net, in_times, in_cells, nsteps: int, workdir: str, trace=(0, 
     """Run the reference EDLUT CPU kernel (oracle/_ref/ref_harness) on the same network.
 
     Returns dict(spike_time, spike_cell, trace[steps, n, nvars], syn (sorted records),
-    w_final (original order), counts)."""
+    w_final (original order), counts, of_text / sf_text (bytes of the reference's
+    output-spike and saved-weights files))."""
     from edlut_b200.network import write_input_spikes
     netf, wf = net.write_files(workdir)
     inp = os.path.join(workdir, "inputs.cfg")
@@ -165,6 +166,12 @@ def run_reference(net, in_times, in_cells, nsteps: int, workdir: str, trace=(0, 
     out["w_final"] = np.frombuffer(raw[8:].tobytes(), np.float32).copy()
     with open(os.path.join(workdir, "out.counts")) as f:
         out["counts"] = [int(x) for x in f.read().split()]
+    # the reference's own output files: spikes (-of) and weights (-sf)
+    for key, ext in (("of_text", ".of"), ("sf_text", ".sf")):
+        path = os.path.join(workdir, "out" + ext)
+        if os.path.exists(path):
+            with open(path, "rb") as f:
+                out[key] = f.read()
     return out
 
 

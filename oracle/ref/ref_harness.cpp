@@ -11,6 +11,8 @@
 //                  reference's sorted synapse order (qsort_inters, Network.cpp:45-68)
 //   <out>.wfinal   int64 m, then m float32 final weights in network-file order
 //   <out>.counts   text: spikes propagated_events
+//   <out>.of       text: the reference's own FileOutputSpikeDriver file (-of)
+//   <out>.sf       text: the reference's own Network::SaveWeights file (-sf)
 //
 // Usage: ref_harness net.cfg weights.cfg inputs.cfg|- nsteps dt_s out_prefix
 //                    [trace_steps trace_first_cell trace_ncells]
@@ -42,6 +44,7 @@
 #include "neuron_model/NeuronModel.h"
 #include "communication/FileInputSpikeDriver.h"
 #include "communication/ArrayOutputSpikeDriver.h"
+#include "communication/FileOutputSpikeDriver.h"
 #undef private
 #undef protected
 
@@ -65,6 +68,8 @@ int main(int argc, char **argv) {
         if (std::strcmp(inp, "-") != 0) sim.AddInputSpikeDriver(new FileInputSpikeDriver(inp));
         ArrayOutputSpikeDriver *outdrv = new ArrayOutputSpikeDriver();
         sim.AddOutputSpikeDriver(outdrv);
+        FileOutputSpikeDriver *filedrv = new FileOutputSpikeDriver((out + ".of").c_str(), false);
+        sim.AddOutputSpikeDriver(filedrv);
         sim.InitSimulation();
 
         Network *nw = sim.GetNetwork();
@@ -125,6 +130,9 @@ int main(int argc, char **argv) {
         std::fwrite(&m, 8, 1, fw);
         for (int64_t j = 0; j < m; ++j) { float w = nw->wordination[j]->GetWeight(); std::fwrite(&w, 4, 1, fw); }
         std::fclose(fw);
+
+        nw->SaveWeights((out + ".sf").c_str());
+        std::fflush(filedrv->Handler);
 
         std::ofstream fc(out + ".counts");
         fc << sim.GetTotalSpikeCounter() << " " << sim.GetTotalPropagateCounter() << "\n";

@@ -29,3 +29,26 @@ def spike_match_fraction(a, b):
     same = len(sa & sb) / len(sa)
     near = sum(1 for (s, c) in sa if (s, c) in sb or (s - 1, c) in sb or (s + 1, c) in sb) / len(sa)
     return same, near
+
+
+def load_golden_text(name, ext):
+    """Bytes of the reference's own output file kept for a case (ext ".of": output
+    spikes, ".sf": saved weights)."""
+    import gzip
+    with gzip.open(os.path.join(GOLDEN, name + ext + ".gz"), "rb") as f:
+        return f.read()
+
+
+def weights_file_text(w):
+    """Network::SaveWeights' format (src/spike/Network.cpp:1165-1202): runs of equal
+    consecutive weights, one "%i %g" line per run."""
+    w = np.asarray(w, np.float32)
+    lines = []
+    i = 0
+    while i < len(w):
+        j = i + 1
+        while j < len(w) and w[j] == w[i]:
+            j += 1
+        lines.append("%i %g\n" % (j - i, float(w[i])))
+        i = j
+    return "".join(lines).encode()

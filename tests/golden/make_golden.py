@@ -9,6 +9,8 @@ Each case is a seeded network from edlut_b200.configs (so tests rebuild the same
 network anywhere); the fixture ``<case>.npz`` holds what the reference produced:
 spike steps and cells, the first state-variable traces of a few neurons, final
 weights (plastic cases), a SHA-256 of the reference synapse order, and counts.
+For FILE_CASES the reference's own output-spike (-of) and saved-weights (-sf)
+files are kept as ``<case>.of.gz`` and ``<case>.sf.gz``.
 """
 from __future__ import annotations
 
@@ -57,6 +59,12 @@ CASES["hh_small_bdf2"] = ("hh_network", dict(n=400, indeg=40, t_end=0.1), 2000, 
 CASES["poisson_lif_rk2_stdp"] = ("poisson_network", dict(seed=6), 2000, (300, 70, 8))
 
 
+# cases whose reference output files (-of spikes, -sf weights) are kept as
+# <case>.of.gz / <case>.sf.gz: one model population, so the reference writes a
+# step's spikes in neuron order
+FILE_CASES = ("adex_rk4_stdp",)
+
+
 def build_case(name: str):
     builder, kw, nsteps, trace = CASES[name]
     net, t, c = getattr(C, builder)(**kw)
@@ -90,6 +98,11 @@ def make(name: str) -> dict:
         out["w_final"] = R["w_final"].astype(np.float32)
     out["perm_sha256"] = np.array(perm_digest(R["syn"]["orig"]))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    if name in FILE_CASES:
+        import gzip
+        for key, ext in (("of_text", ".of.gz"), ("sf_text", ".sf.gz")):
+            with gzip.GzipFile(os.path.join(HERE, name + ext), "wb", mtime=0) as f:
+                f.write(R[key])
     return dict(spikes=int(len(steps)), counts=[int(x) for x in R["counts"]])
 
 

@@ -218,3 +218,55 @@ def test_benchmark_size_properties():
     assert np.all(w[plastic] >= 0) and np.all(w[plastic] <= net.max_weight[plastic])
     np.testing.assert_array_equal(outs[0][0], outs[1][0])
     assert outs[0][2].tobytes() == outs[1][2].tobytes()
+
+
+def test_spike_drains_are_sorted_on_the_device():
+    """eb_get_spikes sorts the recording buffer on the device (a radix sort over
+    the varying bits of step and neuron).  With E_leak above threshold every
+    neuron fires in every step, so each drain is the full (step, neuron) grid of
+    the steps since the previous drain: millions of records over many tiles and
+    digit passes, uneven step ranges, and a one-step drain."""
+    from edlut_b200.network import Layer, NetworkDescription
+    from edlut_b200.configs import LIF_C1
+    n = 70_000
+    net = NetworkDescription()
+    net.add_layer(Layer(n, "LIFTimeDrivenModel", dict(LIF_C1, e_leak=-40.0), integrator="Euler"))
+    sim = make_sim(net, record_capacity=16 << 20)
+    done = 0
+    for run in (37, 200, 1, 8):
+        sim.run(run)
+        st, ce = sim.spikes()
+        steps = np.arange(done + 1, done + run + 1, dtype=np.int64)
+        np.testing.assert_array_equal(st, np.repeat(steps, n))
+        np.testing.assert_array_equal(ce, np.tile(np.arange(n, dtype=np.int64), run))
+        done += run
+    st, ce = sim.spikes()
+    assert len(st) == 0
+    sim.close()
+
+
+def test_output_files_match_the_reference_files(tmp_path):
+    """eb_write_spikes and eb_save_weights write the reference's -of spike file and
+    -sf weights file byte for byte (the reference's own files, kept with the
+    golden fixtures); a population whose output flag is off writes nothing."""
+    from tests._cases import load_golden_text
+    from tests.golden.make_golden import FILE_CASES
+    for name in FILE_CASES:
+        net, t, c, nsteps, trace = build_case(name)
+        sim = make_sim(net)
+        sim.inject_spikes(t, c)
+        sim.run(nsteps // 2)
+        of = str(tmp_path / (name + ".of"))
+        sim.write_spikes(of)
+        sim.run(nsteps - nsteps // 2)
+        sim.write_spikes(of, append=True)
+        sf = str(tmp_path / (name + ".sf"))
+        sim.save_weights(sf)
+        assert open(of, "rb").read() == load_golden_text(name, ".of")
+        assert open(sf, "rb").read() == load_golden_text(name, ".sf")
+        model = next(q for q, l in enumerate(net.layers) if l.model != "InputSpikeNeuronModel")
+        sim.set_output(model, False)
+        sim.run(200)
+        sim.write_spikes(of)
+        assert open(of, "rb").read() == b""
+        sim.close()

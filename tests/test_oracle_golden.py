@@ -40,3 +40,23 @@ def test_delay_rounding_matches_reference_rule(oracle):
     assert oracle.round_delay(0.00005) == 0.0001
     assert oracle.round_delay(0.0) == 0.0001
     assert oracle.round_delay(0.005) == 50 * 0.0001
+
+
+def test_reference_output_files_agree_with_fixture():
+    """The reference's own -of spike file and -sf weights file kept for a case hold
+    the same spikes and weights as its binary fixture: the spike lines are the
+    update times of the fixture's steps (printed with %f) and its neurons in
+    (step, neuron) order; the weights file is the fixture's final weights in the
+    SaveWeights run-length format."""
+    from oracle.oracle import step_times
+    from tests._cases import load_golden_text, weights_file_text
+    from tests.golden.make_golden import FILE_CASES
+    for name in FILE_CASES:
+        g = load_golden(name)
+        net, t, c, nsteps, trace = build_case(name)
+        dt = next(l.dt for l in net.layers if l.model != "InputSpikeNeuronModel")
+        ts = step_times(dt, nsteps)
+        pairs = spike_pairs(g["spike_step"], g["spike_cell"])
+        expect = "".join("%f\t%d\n" % (ts[s], cell) for s, cell in pairs.tolist()).encode()
+        assert load_golden_text(name, ".of") == expect
+        assert load_golden_text(name, ".sf") == weights_file_text(g["w_final"])
