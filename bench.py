@@ -347,6 +347,8 @@ def run_ours(args):
         result["sweep"] = run_sweep(args, rank, world)
     if args.adjoint_networks > 0:
         result["adjoint"] = run_adjoint(args, rank, world)
+    if args.hh_neurons > 0:
+        result["hh"] = run_hh(args, rank, world)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -420,6 +422,54 @@ def run_sweep(args, rank, world):
            "autotune": tune, "device_gb": info["device_bytes"] / 1e9, "timing": "CUDA events, mean of 2 runs"}
     sw.close()
     return out
+
+
+HH_WORKLOAD = ("stiff Hodgkin-Huxley network: HH neurons (Na/K/leak, reference default parameters), fixed in-degree "
+               "100 from uniformly random sources (80/20 E/I), integer delays uniform 1-5 ms, one 200 Hz Poisson "
+               "drive per neuron, BDF order 2 at dt 0.05 ms, fp32 state, 500 ms")
+
+
+def run_hh(args, rank, world):
+    """Stiff HH leg: the whole 500 ms (10,000 BDF2 steps) of the HH network after a
+    short untimed warm-up, device-timed with CUDA events on the simulation stream.
+    Algorithmic bytes per neuron-update: 48 B of HH state (V, m, h, n, gE, gI) plus
+    96 B of BDF2 history, 8 B per delivered event and per fanned-out event."""
+    import torch
+    from edlut_b200.configs import hh_network
+    from edlut_b200.simulation import Simulation
+    dt, warm, nsteps = 5e-5, 200, args.hh_steps
+    net, tin, cin = hh_network(seed=rank_seed(1, rank), n=args.hh_neurons, t_end=(warm + nsteps + 10) * dt,
+                               unique_times=False)
+    n = net.layers[1].n
+    sim = Simulation.from_description(net, record_capacity=16 << 20)
+    sim.inject_spikes(tin, cin)
+    from edlut_b200 import _lib
+    L = _lib.load()
+    _lib.check(L.eb_prestage(sim._h, warm + nsteps))
+    sim.run(warm)
+    sim.spikes()
+    c0 = sim.counters()
+    st = torch.cuda.ExternalStream(ctypes_stream(sim))
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    sim.run_async(nsteps)
+    b.record(st)
+    sim.sync()
+    sec = max_over_ranks(a.elapsed_time(b) / 1e3, world)
+    c1 = sim.counters()
+    events = c1["events"] - c0["events"]
+    spikes = c1["spikes"] - c0["spikes"]
+    alg = (BYTES_PER_UNIT["HH"] + 96) * n * nsteps + EVENT_BYTES * events * 2
+    peak, peak_kind = measured_peaks()
+    sim.close()
+    return {"workload": HH_WORKLOAD, "neurons": n * world, "synapses": int(net.n_synapses) * world,
+            "steps": nsteps, "ms": 1e3 * sec, "us_per_step": 1e6 * sec / nsteps,
+            "neuron_updates_per_s": world * n * nsteps / sec, "syn_events_per_s": world * events / sec,
+            "spikes_per_s": world * spikes / sec, "mean_rate_hz": spikes / n / (nsteps * dt),
+            "alg_bytes_per_step": alg / nsteps, "achieved_gbs": alg / sec / 1e9,
+            "frac": alg / sec / 1e9 / peak, "peak": peak, "peak_source": peak_kind,
+            "timing": "CUDA events around the run on the simulation stream, inputs resident"}
 
 
 ADJOINT_WORKLOAD = ("adjoint fitting: LIF networks of 10k neurons (80/20 E/I, in-degree exactly 100 recurrent + 10 "
@@ -612,6 +662,8 @@ def main():
     ap.add_argument("--sweep-sample", type=int, default=6, help="networks also run alone on the plain path")
     ap.add_argument("--profile-sweep", action="store_true", help="untimed sweep run for an external profiler")
     ap.add_argument("--adjoint-networks", type=int, default=64, help="adjoint leg (0: skip)")
+    ap.add_argument("--hh-neurons", type=int, default=100000, help="stiff HH leg (0: skip)")
+    ap.add_argument("--hh-steps", type=int, default=10000)
     ap.add_argument("--adjoint-neurons", type=int, default=10000)
     ap.add_argument("--adjoint-steps", type=int, default=5000)
     args = ap.parse_args()

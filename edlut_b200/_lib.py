@@ -37,6 +37,7 @@ SIGNATURES = [
     ("eb_set_connectivity", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_i64p, c_i64p, c_f32p, c_i32p,
                                             c_f32p, c_f32p, c_i32p]),
     ("eb_set_bucket_limit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
+    ("eb_set_wide_indegree", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
     ("eb_finalize", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
     ("eb_load_network_files", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p]),
     ("eb_inject_spikes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_f32p, c_i64p]),

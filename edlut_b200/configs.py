@@ -101,7 +101,7 @@ def cerebellar_layer(seed: int = 1, n_granule: int = 250_000, n_mossy: int = 5_0
 def hh_network(seed: int = 1, n: int = 100_000, indeg: int = 100, t_end: float = 0.5,
                dt: float = 5e-5, drive_hz: float = 200.0, w_exc: float = 3.0,
                w_inh: float = 12.0, w_drive: float = 30.0, bdf_order: int = 2,
-               integrator: str = "BDF", params: dict | None = None):
+               integrator: str = "BDF", params: dict | None = None, unique_times: bool = True):
     """Hodgkin-Huxley network: fixed in-degree from uniformly random sources (80% of
     sources excitatory), integer delays of 1-5 ms, one Poisson drive per neuron at
     ``drive_hz`` through a 1 ms excitatory synapse.
@@ -121,7 +121,7 @@ def hh_network(seed: int = 1, n: int = 100_000, indeg: int = 100, t_end: float =
                      np.where(inh, w_inh, w_exc), np.where(inh, w_inh, w_exc), -1)
     net.add_synapses(np.arange(n) + drv.start, np.arange(n) + hh.start, 1e-3, 0, w_drive,
                      w_drive, -1)
-    times, cells = poisson_input_times(rng, n, drive_hz, t_end, dt)
+    times, cells = poisson_input_times(rng, n, drive_hz, t_end, dt, unique=unique_times)
     return net, times, cells + drv.start
 
 

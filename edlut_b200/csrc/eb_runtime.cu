@@ -439,12 +439,15 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         if ((rc = dalloc((void **)&D.spk_count, 2 * sizeof(uint32_t)))) return rc;
         CK(cudaMemsetAsync(D.spk_count, 0, 2 * sizeof(uint32_t), st));
         uint32_t maxcap = 0;
-        int64_t max_plastic = 0;
+        int64_t max_plastic = 0, max_indeg = 0;
         for (int64_t i = p.first; i < p.first + p.n; ++i) {
             maxcap = std::max(maxcap, h_cap[i]);
             max_plastic = std::max(max_plastic, plastic_end[i] - in_ptr[i]);
+            max_indeg = std::max(max_indeg, in_ptr[i + 1] - in_ptr[i]);
         }
-        D.wide = maxcap > 16 ? 1 : 0;
+        // a block per neuron pays off when a step brings many arrivals (in-degree x
+        // rate x dt); the bucket capacity is only the worst case of one step
+        D.wide = maxcap > 16 && max_indeg > wide_indegree ? 1 : 0;
         p.has_plastic_in = max_plastic > 0;
         p.post_chunks = (int)((max_plastic + kPostThreads - 1) / kPostThreads);
         if (p.has_plastic_in) {
@@ -1234,6 +1237,13 @@ int eb_set_connectivity(eb_ctx *ctx, int64_t m, const int64_t *src, const int64_
     ctx->max_weight.assign(max_weight, max_weight + m);
     if (rule) ctx->rule.assign(rule, rule + m);
     else ctx->rule.assign(m, -1);
+    return EB_OK;
+}
+
+int eb_set_wide_indegree(eb_ctx *ctx, int64_t indegree) {
+    if (!ctx || indegree < 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (ctx->finalized) { set_error("eb_set_wide_indegree after eb_finalize"); return EB_ERR_STATE; }
+    ctx->wide_indegree = indegree;
     return EB_OK;
 }
 

@@ -52,6 +52,7 @@ struct eb_ctx {
     std::vector<float> delay, weight, max_weight;
     std::vector<int32_t> stype, rule;
     uint32_t bucket_limit = 8192, input_multiplicity = 2;
+    int64_t wide_indegree = 1024;  // block-per-neuron update above this in-degree (0: whenever a bucket holds > 16)
     uint32_t rng_seed = 1;  // RandomGenerator::srand value (the reference's EDLUTKernel uses 1)
     int64_t rec_cap = 16 << 20;
     // derived

@@ -199,15 +199,16 @@ def write_input_spikes(path: str, times: Sequence[float], cells: Sequence[int]) 
 
 
 def poisson_input_times(rng: np.random.Generator, n_inputs: int, rate_hz, t_end: float,
-                        dt: float = 1e-4, t_start: float = 0.0) -> tuple:
+                        dt: float = 1e-4, t_start: float = 0.0, unique: bool = True) -> tuple:
     """Seeded Poisson spike lists for ``n_inputs`` input neurons, as (times, cells).
 
     Each input spikes in a step of length ``dt`` with probability rate*dt (at most
     once per step), drawn as geometric gaps between spike steps.  Times are float32
     and placed strictly inside a step window (10%..90% of the way between two update
     times) so that no input event coincides with a neuron update; every time is
-    unique, so the reference's order of events at equal time stamps never matters.
-    Sorted by time.
+    unique, so the reference's order of events at equal time stamps never matters
+    (``unique=False`` skips that step, for throughput runs whose inputs are too dense
+    for unique float32 times).  Sorted by time.
     """
     rate = np.broadcast_to(np.asarray(rate_hz, np.float64), (n_inputs,))
     k0 = int(round(t_start / dt))
@@ -233,7 +234,7 @@ def poisson_input_times(rng: np.random.Generator, n_inputs: int, rate_hz, t_end:
     order = np.lexsort((cell, times))
     times, cell = times[order], cell[order]
     # make float32 times unique (nudge collisions up by one ulp)
-    dup = np.nonzero(times[1:] <= times[:-1])[0]
+    dup = np.nonzero(times[1:] <= times[:-1])[0] if unique else []
     while len(dup):
         for i in dup + 1:
             if times[i] <= times[i - 1]:

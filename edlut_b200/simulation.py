@@ -34,7 +34,8 @@ class Simulation:
 
     def __init__(self, device: int = 0, record_capacity: Optional[int] = None,
                  graph_steps: int = 0, bucket_limit: int = 0, input_multiplicity: int = 0,
-                 persistent: bool = False, random_seed: Optional[int] = None):
+                 persistent: bool = False, random_seed: Optional[int] = None,
+                 wide_indegree: Optional[int] = None):
         L = load()
         h = ctypes.c_void_p()
         check(L.eb_ctx_create(device, None, ctypes.byref(h)))
@@ -52,6 +53,8 @@ class Simulation:
             check(L.eb_set_random_seed(h, int(random_seed)))
         if bucket_limit or input_multiplicity:
             check(L.eb_set_bucket_limit(h, int(bucket_limit), int(input_multiplicity)))
+        if wide_indegree is not None:
+            check(L.eb_set_wide_indegree(h, int(wide_indegree)))
 
     # ------------------------------------------------------------ building --
     @classmethod

@@ -93,6 +93,11 @@ int eb_set_connectivity(eb_ctx *ctx, int64_t m, const int64_t *src, const int64_
 /* Per-target bucket capacity limit (arrivals one neuron can take in one step);
  * default min(in-degree x multiplicity, 8192). */
 int eb_set_bucket_limit(eb_ctx *ctx, uint32_t max_per_target, uint32_t input_multiplicity);
+/* Populations whose largest in-degree exceeds `indegree` (default 1024) update
+ * with a block per neuron, the others with a thread per neuron; both give the
+ * same results.  0: a block per neuron whenever one step can bring more than 16
+ * arrivals to a neuron.  Before eb_finalize. */
+int eb_set_wide_indegree(eb_ctx *ctx, int64_t indegree);
 /* Build the device network: sort synapses (qsort_inters order,
  * src/spike/Network.cpp:45-68), build source-major and target-major tables, allocate
  * state, buckets and tables.  *out_sorted_perm (m entries, optional) receives the

@@ -220,6 +220,30 @@ def test_benchmark_size_properties():
     assert outs[0][2].tobytes() == outs[1][2].tobytes()
 
 
+@pytest.mark.slow
+def test_hh_benchmark_size_properties():
+    """Full stiff Hodgkin-Huxley network (100k HH neurons, BDF2 at 0.05 ms, 10.1M
+    synapses with 1-5 ms delays, a 200 Hz drive per neuron): captured graphs of
+    8-step windows give the same spikes and membrane potentials as one launch per
+    step, the network spikes, and a second run is identical."""
+    from edlut_b200.configs import hh_network
+    nsteps = 600
+    net, t, c = hh_network(seed=1, t_end=(nsteps + 10) * 5e-5, unique_times=False)
+    first, n = net.layers[0].n, net.layers[1].n
+    outs = []
+    for graph_steps in (0, 1, 0):
+        sim = make_sim(net, graph_steps=graph_steps)
+        sim.inject_spikes(t, c)
+        sim.run(nsteps)
+        st, ce = sim.spikes()
+        outs.append((spike_pairs(st, ce), sim.get_state(first, n, 0)))
+        sim.close()
+    assert len(outs[0][0]) > 1000
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o[0], outs[0][0])
+        assert o[1].tobytes() == outs[0][1].tobytes()
+
+
 def test_spike_drains_are_sorted_on_the_device():
     """eb_get_spikes sorts the recording buffer on the device (a radix sort over
     the varying bits of step and neuron).  With E_leak above threshold every

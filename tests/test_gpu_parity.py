@@ -30,12 +30,17 @@ def run_gpu(net, t, c, nsteps, trace, **kw):
     return out
 
 
+@pytest.mark.parametrize("kernel", ["default", "block_per_neuron"])
 @pytest.mark.parametrize("persistent", [True, False], ids=["persistent", "graphs"])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_gpu_matches_reference_fixture(name, persistent):
+def test_gpu_matches_reference_fixture(name, persistent, kernel):
+    """kernel "default": a block per neuron only above 1,024 inputs (the Purkinje-
+    type cells); "block_per_neuron": for every population that one step can give
+    more than 16 arrivals, so both update kernels meet every fixture."""
     net, t, c, nsteps, trace = build_case(name)
     g = load_golden(name)
-    r = run_gpu(net, t, c, nsteps, trace, persistent=persistent)
+    r = run_gpu(net, t, c, nsteps, trace, persistent=persistent,
+                wide_indegree=0 if kernel == "block_per_neuron" else None)
     ref = spike_pairs(g["spike_step"], g["spike_cell"])
     same, near = spike_match_fraction(ref, r["spikes"])
     assert same >= 0.999 and near == 1.0, (same, near)
