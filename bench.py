@@ -429,6 +429,9 @@ HH_WORKLOAD = ("stiff Hodgkin-Huxley network: HH neurons (Na/K/leak, reference d
                "drive per neuron, BDF order 2 at dt 0.05 ms, fp32 state, 500 ms")
 
 
+HH_BUCKET_LIMIT = 64
+
+
 def run_hh(args, rank, world):
     """Stiff HH leg: the whole 500 ms (10,000 BDF2 steps) of the HH network after a
     short untimed warm-up, device-timed with CUDA events on the simulation stream.
@@ -441,7 +444,9 @@ def run_hh(args, rank, world):
     net, tin, cin = hh_network(seed=rank_seed(1, rank), n=args.hh_neurons, t_end=(warm + nsteps + 10) * dt,
                                unique_times=False)
     n = net.layers[1].n
-    sim = Simulation.from_description(net, record_capacity=16 << 20)
+    # about 0.5 arrivals per neuron and step: 64 bucket slots per neuron instead of
+    # in-degree x 2 (an overflow would end the run with EB_ERR_OVERFLOW)
+    sim = Simulation.from_description(net, record_capacity=16 << 20, bucket_limit=HH_BUCKET_LIMIT)
     sim.inject_spikes(tin, cin)
     from edlut_b200 import _lib
     L = _lib.load()
@@ -644,6 +649,21 @@ def run_for_profiler(args):
     sim.close()
 
 
+def run_for_profiler_hh(args):
+    """The stiff HH network (``--hh-neurons``) run untimed for an external profiler:
+    `args.prof_warm` warm-up steps then `args.prof_run` steps on the default path."""
+    from edlut_b200.configs import hh_network
+    from edlut_b200.simulation import Simulation
+    n = args.prof_warm + args.prof_run
+    net, tin, cin = hh_network(seed=1, n=args.hh_neurons, t_end=(n + 10) * 5e-5, unique_times=False)
+    sim = Simulation.from_description(net, bucket_limit=HH_BUCKET_LIMIT)
+    sim.inject_spikes(tin, cin)
+    sim.run(args.prof_warm)
+    sim.run(args.prof_run)
+    print(json.dumps({"profile_run_steps": args.prof_run, "counters": sim.counters()}))
+    sim.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -664,11 +684,15 @@ def main():
     ap.add_argument("--adjoint-networks", type=int, default=64, help="adjoint leg (0: skip)")
     ap.add_argument("--hh-neurons", type=int, default=100000, help="stiff HH leg (0: skip)")
     ap.add_argument("--hh-steps", type=int, default=10000)
+    ap.add_argument("--profile-hh", action="store_true", help="untimed stiff-HH run for an external profiler")
     ap.add_argument("--adjoint-neurons", type=int, default=10000)
     ap.add_argument("--adjoint-steps", type=int, default=5000)
     args = ap.parse_args()
     if args.profile_run:
         run_for_profiler(args)
+        return
+    if args.profile_hh:
+        run_for_profiler_hh(args)
         return
     if args.profile_sweep:
         from edlut_b200.configs import sweep_networks

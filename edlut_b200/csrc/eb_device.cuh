@@ -295,12 +295,13 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
                 c[j] = co[0] * dt * aux[j] + co[1] * x[j];
                 for (int q = 1; q < st; ++q) c[j] += co[q + 1] * hist[q - 1][j];
             }
-            // Jacobian: one-sided difference at eps = 0.1 dt (BDFn.h:704-724)
+            // Jacobian: one-sided difference at eps = 0.1 dt (BDFn.h:704-724).  Its
+            // base point is f(pr), already in aux: deriv clamps its argument in
+            // place before evaluating (HH) and clamping twice changes nothing, so
+            // evaluating it again would give the same values bit for bit.
             {
-                float tmp[NV], pos[NV], neg[NV];
-#pragma unroll
-                for (int v = 0; v < NV; ++v) tmp[v] = pr[v];
-                M::deriv(P, tmp, pos, rf);
+                float tmp[NV], neg[NV];
+                const float *pos = aux;
 #pragma unroll
                 for (int j = 0; j < ND; ++j) {
 #pragma unroll

@@ -437,8 +437,12 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
 // launch of one step keeps the population spike list (with several, no kernel
 // reads it: fan-out is done here and post-synaptic STDP is deferred).
 // push_inv_dt > 0: also fan out the spikes (1 / step, for arrival_step).
+// HH under BDF holds the Newton state (Jacobian, inverse, history) in about 120
+// registers, which leaves 2 blocks per SM; bounded to 3 blocks (80 registers, a
+// 44-byte spill) a 100k-neuron population fits one wave and its steps take a
+// quarter less time.  Every other instantiation keeps the compiler's choice.
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kNarrowTile) k_update_narrow(PopDev P, NetDev N, int rel, int nsteps,
+__global__ void __launch_bounds__(kNarrowTile, (KIND == KIND_HH && INTEG == INTEG_BDF) ? 3 : 0) k_update_narrow(PopDev P, NetDev N, int rel, int nsteps,
                                                                 double push_inv_dt) {
     const int64_t k = cur_step(N, rel);
     const bool list = nsteps == 1;
