@@ -75,10 +75,22 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML queries every 5 ms from a thread (read-only), or nvidia-smi at
+    its 200 ms period where NVML cannot be opened."""
+
+    # nvmlClocksEventReason* bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu_index: int):
         self.proc = None
+        self.thread = None
+        self.samples = []
+        try:
+            self._start_nvml(gpu_index)
+            return
+        except Exception:
+            self.thread = None
         self.path = tempfile.mktemp(prefix="clocks_", suffix=".csv")
         if shutil.which("nvidia-smi"):
             q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -89,7 +101,44 @@ class ClockSampler:
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
 
+    def _start_nvml(self, gpu_index: int):
+        import threading
+        import pynvml as nv
+        import torch
+        nv.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(gpu_index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            h = nv.nvmlDeviceGetHandleByIndex(gpu_index)
+        self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        self.stop_flag = threading.Event()
+
+        def loop():
+            while not self.stop_flag.is_set():
+                try:
+                    self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(reasons(h))))
+                except Exception:
+                    pass
+                self.stop_flag.wait(0.005)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
+
     def stop(self):
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            if not self.samples:
+                return None
+            found = set()
+            for _, bits in self.samples:
+                found |= {n for n, b in self.REASONS.items() if bits & b}
+            return {"sm_mhz": statistics.median(m for m, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(found), "samples": len(self.samples), "source": "NVML every 5 ms"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -116,7 +165,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi every 200 ms"}
 
 
 def build_workload(seed: int, t_end: float, scale: float = 1.0):
