@@ -366,7 +366,7 @@ def run_ours(args):
     # cpu baseline (rank 0 only, N=1): reference CPU kernel on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference_sample(args, steps=args.cpu_sample_steps)
+        cpu = cpu_reference_sample(args)
 
     result = {
         "metric": METRIC, "value": world * updates_rank / sec, "unit": UNIT, "n_gpus": world,
@@ -604,78 +604,124 @@ def ctypes_stream(sim):
 
 
 # ------------------------------------------------------- reference arm ----
-def ref_binary():
-    p = os.path.join(ROOT, "oracle", "_ref", "EDLUTKernel")
+REF_WARM_STEPS = 500       # reference run-in before its timed samples (past the start-up transient)
+REF_SINGLE_SAMPLES = 2     # samples of the 1-thread reference run
+
+
+def ref_binary(name="ref_bench"):
+    p = os.path.join(ROOT, "oracle", "_ref", name)
     return p if os.path.exists(p) else None
 
 
-def cpu_reference_sample(args, steps: int, threads: int | None = None):
-    """Time the reference EDLUT CPU kernel (EDLUTKernel, -openmp Q) on a bounded
-    sample of the workload: the cerebellar layer at 1/10 scale (25k granule AdEx,
-    500 mossy fibres, 20 Purkinje x 5k plastic synapses), `steps` integration steps.
-    Setup is removed by subtracting a 1-step run.  Falls back to the C oracle port
-    (single thread) when the reference build is absent."""
-    scale = 0.1
-    t_end = (steps + 20) * DT
-    net, tin, cin = build_workload(seed=11, t_end=t_end, scale=scale)
-    n_model = sum(l.n for l in net.layers if l.model != "InputSpikeNeuronModel")
-    exe = ref_binary()
-    cores = threads or os.cpu_count() or 1
-    if exe is None:
-        from oracle import oracle as O
-        t0 = time.perf_counter()
-        r = O.run(net, tin, cin, steps)
-        el = time.perf_counter() - t0
-        return {"value": n_model * steps / el, "unit": UNIT, "cores": 1, "kind": "port",
-                "sample": "C oracle port, cerebellar layer at 1/10 scale, %d steps" % steps,
-                "syn_events_per_s": r["n_events"] / el}
-    from edlut_b200.network import write_input_spikes
-    wd = tempfile.mkdtemp(prefix="edlut_ref_")
-    netf, wf = net.write_files(wd)
-    write_input_spikes(os.path.join(wd, "inputs.cfg"), tin, cin)
+class ReferenceWorkload:
+    """The benchmark network written once in the reference's file formats (network,
+    weights, model .cfg and input-spike files) for the reference's own CPU kernel:
+    the same builder, seed and size as the GPU arm's rank 0."""
 
-    def run(nst):
-        cmd = [exe, "-time", repr(nst * DT + 0.5 * DT), "-nf", os.path.basename(netf), "-wf",
-               os.path.basename(wf), "-if", "inputs.cfg", "-openmp", str(cores)]
-        t0 = time.perf_counter()
-        r = subprocess.run(cmd, cwd=wd, capture_output=True, text=True)
-        el = time.perf_counter() - t0
+    def __init__(self, steps_needed: int, seed: int = 1, scale: float = 1.0):
+        from edlut_b200.network import write_input_spikes
+        net, tin, cin = build_workload(seed=seed, t_end=(steps_needed + 20) * DT, scale=scale)
+        self.n_model = sum(l.n for l in net.layers if l.model != "InputSpikeNeuronModel")
+        self.dir = tempfile.mkdtemp(prefix="edlut_ref_")
+        self.netf, self.wf = (os.path.basename(p) for p in net.write_files(self.dir))
+        write_input_spikes(os.path.join(self.dir, "inputs.cfg"), tin, cin)
+        self.scale = scale
+
+    def time(self, threads: int, warm: int, sample_steps: int, samples: int) -> dict:
+        """Run oracle/_ref/ref_bench (the reference's Simulation with `threads` OpenMP
+        queues): set-up and `warm` steps untimed, then `samples` timed samples of
+        `sample_steps` integration steps each, wall clock per sample."""
+        cmd = [ref_binary(), self.netf, self.wf, "inputs.cfg", str(threads), repr(float(np.float32(DT))),
+               str(warm), str(sample_steps), str(samples)]
+        r = subprocess.run(cmd, cwd=self.dir, capture_output=True, text=True)
         if r.returncode != 0:
-            raise RuntimeError("EDLUTKernel failed: " + r.stdout[-500:] + r.stderr[-500:])
-        ev = 0
-        for line in r.stdout.splitlines():
-            if line.startswith("Total Propagated Spikes and Events"):
-                ev = int(line.split(":")[1].split(",")[0])
-        return el, ev
-    t1, _ = run(1)
-    tn, ev = run(steps)
-    shutil.rmtree(wd, ignore_errors=True)
-    sim_s = max(tn - t1, 1e-9)
-    return {"value": n_model * (steps - 1) / sim_s, "unit": UNIT, "cores": cores, "kind": "reference",
-            "sample": "reference EDLUTKernel -openmp %d, cerebellar layer at 1/10 scale (%d neurons), %d steps, "
-                      "setup removed by subtracting a 1-step run" % (cores, n_model, steps),
-            "syn_events_per_s": ev / sim_s}
+            raise RuntimeError("ref_bench failed: " + r.stdout[-500:] + r.stderr[-500:])
+        out = json.loads(r.stdout.strip().splitlines()[-1])
+        out["value"] = [self.n_model * sample_steps / s for s in out["sample_s"]]
+        out["events_per_s"] = [e / s for e, s in zip(out["events"], out["sample_s"])]
+        return out
+
+    def close(self):
+        shutil.rmtree(self.dir, ignore_errors=True)
+
+
+def ref_sample_text(threads: int, n_model: int, warm: int, per: int, n: int, scale: float) -> str:
+    size = "full size" if scale == 1.0 else "scale %g" % scale
+    return ("reference EDLUT CPU kernel (its Simulation class, %d OpenMP queue%s), the benchmark's cerebellar "
+            "network at %s (%d model neurons, same seed and inputs), %d samples of %d integration steps after "
+            "%d untimed steps; set-up excluded" % (threads, "s" if threads > 1 else "", size, n_model, n, per,
+                                                     warm, ))
+
+
+def cpu_reference_sample(args, samples: int = 3):
+    """CPU baseline of the GPU arm: the reference's own CPU kernel on the same
+    workload, all host cores and one thread, a few samples each.  Falls back to the
+    C oracle port (single thread, 1/10 scale) when the reference build is absent."""
+    per = args.cpu_sample_steps
+    cores = os.cpu_count() or 1
+    if ref_binary() is None:
+        from oracle import oracle as O
+        net, tin, cin = build_workload(seed=1, t_end=(per + 20) * DT, scale=0.1)
+        n_model = sum(l.n for l in net.layers if l.model != "InputSpikeNeuronModel")
+        t0 = time.perf_counter()
+        r = O.run(net, tin, cin, per)
+        el = time.perf_counter() - t0
+        return {"value": n_model * per / el, "unit": UNIT, "cores": 1, "kind": "port",
+                "sample": "C oracle port, cerebellar layer at 1/10 scale, %d steps" % per,
+                "syn_events_per_s": r["n_events"] / el, "same_config": False}
+    wl = ReferenceWorkload(REF_WARM_STEPS + per * samples, scale=args.scale)
+    try:
+        allc = wl.time(cores, REF_WARM_STEPS, per, samples)
+        one = wl.time(1, REF_WARM_STEPS, per, REF_SINGLE_SAMPLES)
+    finally:
+        wl.close()
+    return {"value": statistics.mean(allc["value"]), "unit": UNIT, "cores": allc["queues"], "kind": "reference",
+            "sample": ref_sample_text(allc["queues"], wl.n_model, REF_WARM_STEPS, per, samples, args.scale),
+            "syn_events_per_s": statistics.mean(allc["events_per_s"]), "same_config": args.scale == 1.0,
+            "setup_s": allc["setup_s"],
+            "single_thread": {"value": statistics.mean(one["value"]), "cores": 1,
+                              "syn_events_per_s": statistics.mean(one["events_per_s"]),
+                              "sample": ref_sample_text(1, wl.n_model, REF_WARM_STEPS, per, REF_SINGLE_SAMPLES,
+                                                        args.scale)}}
 
 
 def run_reference(args):
+    """Reference arm: the reference's own CPU kernel (oracle/_ref/ref_bench, built
+    from the reference sources) on the GPU arm's workload, every host core; each
+    benchmark step is one sample of --cpu-sample-steps integration steps of the one
+    loaded network (set-up once, untimed).  A 1-thread run is reported beside it."""
     rank, world, _ = env_rank()
     if rank != 0:
         return
-    samples = []
     W, K = args.warmup, args.steps
-    for i in range(W + K):
-        r = cpu_reference_sample(args, steps=args.cpu_sample_steps)
-        if i >= W:
-            samples.append(r)
-    v = statistics.mean(s["value"] for s in samples)
-    ev = statistics.mean(s["syn_events_per_s"] for s in samples)
+    per = args.cpu_sample_steps
+    cores = os.cpu_count() or 1
+    if ref_binary() is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU kernel not built (oracle/_ref/ref_bench)"}))
+        return
+    wl = ReferenceWorkload(REF_WARM_STEPS + per * (W + K), scale=args.scale)
+    try:
+        allc = wl.time(cores, REF_WARM_STEPS + per * W, per, K)
+        one = wl.time(1, REF_WARM_STEPS, per, REF_SINGLE_SAMPLES)
+    finally:
+        wl.close()
+    v = statistics.mean(allc["value"])
+    ev = statistics.mean(allc["events_per_s"])
+    sample = ref_sample_text(allc["queues"], wl.n_model, REF_WARM_STEPS + per * W, per, K, args.scale)
     result = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": K,
-              "warmup": W, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-              "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-              "config": {"workload": WORKLOAD, "sample": samples[0]["sample"]},
+              "warmup": W, "ms_per_step": 1e3 * statistics.mean(allc["sample_s"]), "higher_is_better": True,
+              "scaling": "weak", "vs_baseline": None, "dtype": "f32 (state), f64 (event times)",
+              "data": "synthetic (seeded Poisson mossy-fibre inputs, random connectivity)",
+              "config": {"workload": WORKLOAD, "integration_steps_per_step": per, "neurons": wl.n_model,
+                         "scale": args.scale, "sample": sample},
               "syn_events_per_s": ev,
-              "cpu_baseline": {"value": v, "unit": UNIT, "cores": samples[0]["cores"], "kind": samples[0]["kind"],
-                               "sample": samples[0]["sample"]},
+              "cpu_baseline": {"value": v, "unit": UNIT, "cores": allc["queues"], "kind": "reference",
+                               "sample": sample},
+              "single_thread": {"value": statistics.mean(one["value"]), "cores": 1,
+                                "syn_events_per_s": statistics.mean(one["events_per_s"]),
+                                "sample": ref_sample_text(1, wl.n_model, REF_WARM_STEPS, per, REF_SINGLE_SAMPLES,
+                                                          args.scale)},
+              "setup_s": allc["setup_s"], "host_cores": cores,
               "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(result))
 
@@ -720,7 +766,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--cpu-sample-steps", type=int, default=2000)
+    ap.add_argument("--cpu-sample-steps", type=int, default=50,
+                    help="integration steps per reference CPU sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-run", action="store_true", help="untimed run for an external profiler")
     ap.add_argument("--prof-warm", type=int, default=300)

@@ -178,14 +178,31 @@ class NetworkDescription:
             for name, params in self.rules:
                 f.write("%s %s\n" % (name, " ".join(_f32(v) for v in params)))
             f.write("%d\n" % self.n_synapses)
-            lines = []
-            for s, t, d, ty, mw, wc in zip(self.src.tolist(), self.tgt.tolist(),
-                                            self.delay.tolist(), self.stype.tolist(),
-                                            self.max_weight.tolist(), self.wchange.tolist()):
-                lines.append("%d 1 %d 1 1 %s 0 %d %s %d\n" % (s, t, _f32(d), ty, _f32(mw), wc))
-            f.writelines(lines)
+            # the line after "src 1 tgt 1 1" is shared by every synapse with the same
+            # delay, type, max weight and rule: format each distinct one once
+            cols = [np.unique(a, return_inverse=True) for a in
+                    (self.delay.astype(np.float32), self.stype, self.max_weight.astype(np.float32), self.wchange)]
+            key = np.zeros(self.n_synapses, np.int64)
+            for u, inv in cols:
+                key = key * len(u) + inv.reshape(-1)
+            ukey, code = np.unique(key, return_inverse=True)
+            tails = []
+            for k in ukey.tolist():
+                idx = []
+                for u, _ in reversed(cols):
+                    idx.append(k % len(u))
+                    k //= len(u)
+                (d, ty, mw, wc) = (cols[j][0][i] for j, i in enumerate(reversed(idx)))
+                tails.append(" %s 0 %d %s %d\n" % (_f32(d), int(ty), _f32(mw), int(wc)))
+            for lo in range(0, self.n_synapses, 1 << 20):
+                hi = min(self.n_synapses, lo + (1 << 20))
+                f.writelines(["%d 1 %d 1 1%s" % (s, t, tails[c]) for s, t, c in
+                              zip(self.src[lo:hi].tolist(), self.tgt[lo:hi].tolist(),
+                                  code.reshape(-1)[lo:hi].tolist())])
         with open(wf, "w") as f:
-            f.writelines("1 %s\n" % _f32(w) for w in self.weight.tolist())
+            w32 = self.weight.astype(np.float32)
+            for lo in range(0, len(w32), 1 << 20):
+                f.writelines(["1 %s\n" % v for v in np.char.mod("%.9g", w32[lo:lo + (1 << 20)].astype(np.float64)).tolist()])
         return netf, wf
 
 

@@ -1,9 +1,11 @@
 """Generate the golden fixtures under tests/golden/ by running the reference EDLUT
-CPU kernel (built from the reference sources by ``make -C oracle ref``; needs the
-reference tree, so this runs only where it is mounted).
+CPU kernel (built from the reference sources by
+``make -C oracle ref REF=<reference tree>/Kernel``, so this runs only where the
+reference is mounted).
 
-    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py            # all small cases
     python tests/golden/make_golden.py c1_lif     # cases whose name contains 'c1_lif'
+    python tests/golden/make_golden.py full       # the full-size benchmark cases (minutes)
 
 Each case is a seeded network from edlut_b200.configs (so tests rebuild the same
 network anywhere); the fixture ``<case>.npz`` holds what the reference produced:
@@ -34,7 +36,8 @@ CASES = {
     "c1_lif_euler": ("lif_recurrent", {}, 10000, (1000, 100, 16)),
 }
 for _m in ("LIFTimeDrivenModel", "AdExTimeDrivenModel", "HHTimeDrivenModel"):
-    for _i, _o in (("Euler", 1), ("RK2", 1), ("RK4", 1), ("BDF", 1), ("BDF", 2), ("BDF", 3)):
+    for _i, _o in (("Euler", 1), ("RK2", 1), ("RK4", 1), ("BDF", 1), ("BDF", 2), ("BDF", 3), ("BDF", 4),
+                   ("BDF", 5), ("BDF", 6)):
         _dt = 5e-5 if _m.startswith("HH") else 1e-4
         CASES["%s_%s%s_stdp" % (_m[:-15].lower(), _i.lower(), _o if _i == "BDF" else "")] = (
             "parity_network", dict(model=_m, integrator=_i, bdf_order=_o, stdp=True,
@@ -43,9 +46,18 @@ for _m in ("LIFTimeDrivenModel", "AdExTimeDrivenModel", "HHTimeDrivenModel"):
 CASES["lif_subdt_delays"] = ("parity_network", dict(model="LIFTimeDrivenModel", integrator="Euler",
                                                     delays=(1.5e-4, 1.49e-3, 2.3e-4), dt=1e-4, seed=3),
                              2000, (300, 40, 8))
+# a 1 ms step with weights small enough that RK2 stays stable: finite dynamics
 CASES["lif_coarse_dt"] = ("parity_network", dict(model="LIFTimeDrivenModel", integrator="RK2",
-                                                 delays=(1e-4, 2e-4, 5e-4), dt=1e-3, seed=4, t_end=1.0),
+                                                 delays=(1e-4, 2e-4, 5e-4), dt=1e-3, seed=4, t_end=1.0,
+                                                 weights=dict(w_in=0.15, w_exc=0.05, w_inh=0.2)),
                           1000, (300, 40, 8))
+# the same step with the default weights: conductances past the explicit methods'
+# stability bound, so V overflows to inf and NaN, which both sides must propagate
+# (and reset) identically
+CASES["lif_coarse_dt_overflow"] = ("parity_network", dict(model="LIFTimeDrivenModel", integrator="RK2",
+                                                          delays=(1e-4, 2e-4, 5e-4), dt=1e-3, seed=4,
+                                                          t_end=1.0),
+                                   1000, (300, 40, 8))
 CASES["adex_dense_fanin"] = ("parity_network", dict(model="AdExTimeDrivenModel", integrator="RK4", n=120,
                                                     p=0.6, stdp=True, seed=5, delays=(1e-3,)),
                              2000, (300, 40, 8))
@@ -56,7 +68,25 @@ CASES["hh_small_bdf2"] = ("hh_network", dict(n=400, indeg=40, t_end=0.1), 2000, 
 # device Poisson generators (PoissonGeneratorDeviceVector): two generator types, one
 # of them split around the LIF layer (its seeds follow the first part's), STDP on
 # the generator synapses
-CASES["poisson_lif_rk2_stdp"] = ("poisson_network", dict(seed=6), 2000, (300, 70, 8))
+CASES["poisson_lif_rk2_stdp"] = ("poisson_network", dict(seed=6, w_in=0.05, w_exc=0.05, w_inh=0.5), 2000,
+                                 (300, 70, 8))
+
+# Fixtures that may hold non-finite state on purpose (every other fixture's traces
+# are finite).
+OVERFLOW_CASES = ("lif_coarse_dt_overflow",)
+
+# The benchmark workloads at full size, over the first steps of their runs.  Their
+# fixtures keep the spikes, the V traces of a few cells, counts and SHA-256 digests
+# of the synapse order and of the final weights (with every 997th weight), instead
+# of whole weight arrays.
+#   c2_full_rk4: cerebellar layer, 250k AdEx granule + 200 LIF Purkinje x 50k
+#                plastic synapses, RK4 at 0.1 ms; traces of 8 Purkinje cells
+#   c3_full_bdf2: 100k HH neurons, in-degree 100, delays 1-5 ms, 200 Hz drive,
+#                BDF2 at 0.05 ms, unique input times; traces of 8 HH cells
+BIG_CASES = {
+    "c2_full_rk4": ("cerebellar_layer", dict(t_end=0.052), 500, (500, 255000, 8)),
+    "c3_full_bdf2": ("hh_network", dict(t_end=0.0102), 200, (200, 100000, 8)),
+}
 
 
 # cases whose reference output files (-of spikes, -sf weights) are kept as
@@ -66,7 +96,7 @@ FILE_CASES = ("adex_rk4_stdp",)
 
 
 def build_case(name: str):
-    builder, kw, nsteps, trace = CASES[name]
+    builder, kw, nsteps, trace = CASES[name] if name in CASES else BIG_CASES[name]
     net, t, c = getattr(C, builder)(**kw)
     return net, t, c, nsteps, trace
 
@@ -81,7 +111,29 @@ def step_of_times(times: np.ndarray, dt: float, nsteps: int) -> np.ndarray:
     return np.searchsorted(mid, times)
 
 
+def weights_digest(w: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(w, np.float32).tobytes()).hexdigest()
+
+
+def make_big(name: str) -> dict:
+    net, t, c, nsteps, trace = build_case(name)
+    dt = next(l.dt for l in net.layers if l.model != "InputSpikeNeuronModel")
+    with tempfile.TemporaryDirectory() as wd:
+        R = O.run_reference(net, t, c, nsteps, wd, trace=trace)
+    steps = step_of_times(R["spike_time"], dt, nsteps)
+    order = np.lexsort((R["spike_cell"], steps))
+    w = R["w_final"].astype(np.float32)
+    out = dict(spike_step=steps[order].astype(np.int32), spike_cell=R["spike_cell"][order].astype(np.int32),
+               trace=R["trace"][:, :, :1].astype(np.float32), counts=np.array(R["counts"], np.int64),
+               perm_sha256=np.array(perm_digest(R["syn"]["orig"])), w_sha256=np.array(weights_digest(w)),
+               w_sample=w[::997].copy())
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    return dict(spikes=int(len(steps)), counts=[int(x) for x in R["counts"]])
+
+
 def make(name: str) -> dict:
+    if name in BIG_CASES:
+        return make_big(name)
     net, t, c, nsteps, trace = build_case(name)
     dt = next(l.dt for l in net.layers if l.model != "InputSpikeNeuronModel")
     with tempfile.TemporaryDirectory() as wd:
@@ -108,11 +160,11 @@ def make(name: str) -> dict:
 
 if __name__ == "__main__":
     if not O.ref_available():
-        sys.exit("reference build missing: run `make -C oracle ref` where the reference tree is mounted")
+        sys.exit("reference build missing: run `make -C oracle ref REF=<reference tree>/Kernel`")
     sel = sys.argv[1:]
     summary = {}
-    for name in CASES:
-        if sel and not any(s in name for s in sel):
+    for name in list(CASES) + list(BIG_CASES):
+        if (sel and not any(s in name for s in sel)) or (not sel and name in BIG_CASES):
             continue
         summary[name] = make(name)
         print(name, summary[name], flush=True)

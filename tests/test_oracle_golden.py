@@ -60,3 +60,15 @@ def test_reference_output_files_agree_with_fixture():
         expect = "".join("%f\t%d\n" % (ts[s], cell) for s, cell in pairs.tolist()).encode()
         assert load_golden_text(name, ".of") == expect
         assert load_golden_text(name, ".sf") == weights_file_text(g["w_final"])
+
+
+def test_fixture_dynamics_are_finite():
+    """Every fixture's traces stay finite except the cases kept to pin overflow
+    (their inf / NaN propagation and reset must match too)."""
+    from tests.golden.make_golden import OVERFLOW_CASES
+    for name in CASES:
+        tr = load_golden(name)["trace"]
+        if name in OVERFLOW_CASES:
+            assert not np.isfinite(tr).all(), name
+        else:
+            assert np.isfinite(tr).all(), name
