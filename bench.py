@@ -420,8 +420,12 @@ def run_sweep(args, rank, world):
     from edlut_b200.configs import sweep_networks
     from edlut_b200.simulation import Simulation
     from edlut_b200.sweep import Sweep
+    from edlut_b200.shard import network_cost, partition
     nsteps = args.sweep_steps
-    specs = sweep_networks(seed=rank_seed(1, rank), n_networks=args.sweep_networks, t_end=nsteps * DT)
+    all_specs = sweep_networks(seed=1, n_networks=args.sweep_networks, t_end=nsteps * DT)
+    # the networks are independent: each rank runs its cost-balanced slice
+    lo, hi = partition([network_cost(sp) for sp in all_specs], world)[rank]
+    specs = all_specs[lo:hi]
     sw = Sweep.from_specs(specs, n_steps_max=nsteps)
     tune = sw.autotune(min(500, nsteps))
     stream = torch.cuda.ExternalStream(sw.stream())
@@ -439,6 +443,11 @@ def run_sweep(args, rank, world):
     sec = max_over_ranks(sec, world)
     info = sw.info()
     sizes = np.array([sp["n"] for sp in specs])
+    tot = torch.tensor([float(sizes.sum()), float(info["synapses"]), float(info["events"])], dtype=torch.float64,
+                       device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(tot)
+    tot_neurons, tot_syn, tot_events = (float(v) for v in tot.tolist())
     # plain path, one network at a time, on networks spread over the size range
     sample = np.argsort(sizes)[np.linspace(0, len(sizes) - 1, args.sweep_sample).astype(int)]
     plain_s, identical = 0.0, True
@@ -460,12 +469,13 @@ def run_sweep(args, rank, world):
         identical &= bool(len(s1) == len(s2) and np.array_equal(s1, s2) and np.array_equal(c1, c2))
         sim.close()
     plain_nps = len(sample) / plain_s
-    nps = world * len(specs) / sec
-    out = {"workload": SWEEP_WORKLOAD, "networks": len(specs) * world, "steps": nsteps,
-           "neurons": int(sizes.sum()) * world, "synapses": info["synapses"] * world,
+    nps = len(all_specs) / sec
+    out = {"workload": SWEEP_WORKLOAD, "networks": len(all_specs), "steps": nsteps,
+           "neurons": int(tot_neurons), "synapses": int(tot_syn),
            "ms": 1e3 * sec, "networks_per_s": nps,
-           "neuron_updates_per_s": world * int(sizes.sum()) * nsteps / sec,
-           "syn_events_per_s": world * info["events"] / sec,
+           "neuron_updates_per_s": tot_neurons * nsteps / sec,
+           "syn_events_per_s": tot_events / sec,
+           "scaling": "strong (the networks split across ranks)" if world > 1 else "single",
            "plain_loop_networks_per_s": plain_nps, "speedup_vs_plain_loop": nps / world / plain_nps,
            "plain_loop_sample": int(len(sample)), "identical_spikes_in_sample": identical,
            "autotune": tune, "device_gb": info["device_bytes"] / 1e9, "timing": "CUDA events, mean of 2 runs"}
@@ -540,13 +550,18 @@ def run_adjoint(args, rank, world):
     import torch
     from edlut_b200.adjoint import TraceModel
     from edlut_b200.configs import adjoint_networks, perturbed_params
-    B, n, steps, every = args.adjoint_networks, args.adjoint_neurons, args.adjoint_steps, 100
-    specs = adjoint_networks(seed=rank_seed(7, rank), n_networks=B, n=n, t_end=steps * DT)
-    obs = np.stack([np.random.default_rng([7, i]).choice(n, 256, replace=False) for i in range(B)])
+    from edlut_b200.shard import network_cost, partition
+    B_all, n, steps, every = args.adjoint_networks, args.adjoint_neurons, args.adjoint_steps, 100
+    all_specs = adjoint_networks(seed=7, n_networks=B_all, n=n, t_end=steps * DT)
+    # independent networks: each rank fits its slice of the batch
+    lo, hi = partition([network_cost(sp) for sp in all_specs], world)[rank]
+    specs = all_specs[lo:hi]
+    B = len(specs)
+    obs = np.stack([np.random.default_rng([7, i]).choice(n, 256, replace=False) for i in range(lo, hi)])
     model = TraceModel(specs, steps, obs, integrator="RK2", checkpoint_every=every)
     rng = np.random.default_rng(99)
     truth = np.array([[perturbed_params(s["params"], rng)[k] for k in ("g_leak", "e_leak", "tau_exc", "tau_inh")]
-                      for s in specs])
+                      for s in all_specs])[lo:hi]
     w0 = model.initial_weights()
     with torch.no_grad():
         target = model(torch.tensor(truth), w0).clone()
@@ -583,12 +598,13 @@ def run_adjoint(args, rank, world):
     gp = params.grad.numpy()
     gw = weights.grad
     info = model.sweep.info()
-    out = {"workload": ADJOINT_WORKLOAD, "networks": B, "neurons_per_network": n, "steps": steps,
+    out = {"workload": ADJOINT_WORKLOAD, "networks": B_all, "networks_per_rank": B, "neurons_per_network": n,
+           "steps": steps, "scaling": "strong (the batch split across ranks)" if world > 1 else "single",
            "checkpoint_every": every, "observed_per_network": 256, "weights": int(model.n_weights),
            "forward_ms": 1e3 * t_f, "forward_backward_ms": 1e3 * t_fb, "cost_ratio": t_fb / t_f,
            "backward_over_forward": (t_fb - t_f) / t_f, "loss": loss,
            "grad_params_norm": float(np.linalg.norm(gp)), "grad_w_norm": float(torch.linalg.norm(gw)),
-           "neuron_updates_per_s_forward": B * n * steps / t_f, "device_gb": info["device_bytes"] / 1e9,
+           "neuron_updates_per_s_forward": B_all * n * steps / t_f, "device_gb": info["device_bytes"] / 1e9,
            "timing": "CUDA events around the whole call (host parameter upload, forward kernels, trace copy; "
                      "backward adds recompute + adjoint kernels), best of 2"}
     model.sweep.close()

@@ -57,18 +57,27 @@ struct File {
     }
 };
 
-// RandomGenerator of the reference: 31-bit LCG, per-generator state seeded from a
-// global chain (RandomGenerator.cpp:21-27).
+// RandomGenerator of the reference: 31-bit LCG whose state is seeded from a seed
+// chain -- each generator takes the chain's value, which then advances
+// (RandomGenerator.cpp:21-27, include/simulation/RandomGenerator.h:61-68).  The
+// reference keeps the chain in a process-global; here each load has its own, so
+// contexts loading networks on different threads do not share it.
+struct SeedChain {
+    unsigned long seed;
+    unsigned long take() {
+        const unsigned long s = seed;
+        seed = ((seed * 765426813) + 54321) & 0x7fffffff;
+        return s;
+    }
+};
 struct RefRandom {
-    static unsigned long global_seed;
     unsigned long next;
-    RefRandom() : next(global_seed) { global_seed = ((global_seed * 765426813) + 54321) & 0x7fffffff; }
+    explicit RefRandom(SeedChain &chain) : next(chain.take()) {}
     float frand() {
         next = ((next * 1103515245) + 12345) & 0x7fffffff;
         return ((float)next) / 2147483647;
     }
 };
-unsigned long RefRandom::global_seed = 1;
 
 const char *kModelNames[] = {"InputSpikeNeuronModel", "LIFTimeDrivenModel", "AdExTimeDrivenModel",
                              "HHTimeDrivenModel", "PoissonGeneratorDeviceVector"};
@@ -223,8 +232,8 @@ extern "C" int eb_load_network_files(eb_ctx *ctx, const char *network_file, cons
     // weights file
     File g(weights_file);
     if (!g.fh) { set_error("cannot open weights file %s", weights_file); return EB_ERR_PARSE; }
-    RefRandom::global_seed = ctx->rng_seed & 0x7fffffffu;
-    RefRandom rnd;
+    SeedChain chain{ctx->rng_seed & 0x7fffffffu};
+    RefRandom rnd(chain);
     g.skip_comments();
     for (long c = 0; c < ninters;) {
         g.skip_comments();

@@ -604,6 +604,30 @@ int eb_ctx::stage_inputs(int64_t k0, int64_t k_end) {
         else rest.push_back(p);
     }
     pending.swap(rest);
+    // After eb_restore, new inputs can precede inputs staged for the abandoned
+    // timeline: merge them into the staged list in time order and re-stage it.
+    if (!nt.empty() && !in_times_host.empty() && nt.front() < in_times_host.back()) {
+        std::vector<double> mt;
+        std::vector<uint32_t> mc;
+        mt.reserve(in_times_host.size() + nt.size());
+        mc.reserve(in_times_host.size() + nt.size());
+        size_t a = 0, b = 0;
+        while (a < in_times_host.size() || b < nt.size()) {
+            if (b == nt.size() || (a < in_times_host.size() && in_times_host[a] <= nt[b])) {
+                mt.push_back(in_times_host[a]);
+                mc.push_back(in_cells_host[a++]);
+            } else {
+                mt.push_back(nt[b]);
+                mc.push_back(nc[b++]);
+            }
+        }
+        in_times_host.clear();
+        in_cells_host.clear();
+        in_total = 0;
+        nt.swap(mt);
+        nc.swap(mc);
+        staged_until = k_end;  // input ranges of later steps are recomputed when they are staged
+    }
     if (!nt.empty()) {
         int64_t need = in_total + (int64_t)nt.size();
         if (need > in_cap) {
@@ -625,6 +649,7 @@ int eb_ctx::stage_inputs(int64_t k0, int64_t k_end) {
         CK(cudaMemcpyAsync(d_in_time + in_total, nt.data(), sizeof(double) * nt.size(), cudaMemcpyHostToDevice, stream));
         CK(cudaMemcpyAsync(d_in_cell + in_total, nc.data(), sizeof(uint32_t) * nc.size(), cudaMemcpyHostToDevice, stream));
         in_times_host.insert(in_times_host.end(), nt.begin(), nt.end());
+        in_cells_host.insert(in_cells_host.end(), nc.begin(), nc.end());
         in_total += (int64_t)nt.size();
     }
     // in_start[k] = first staged input with time >= t_{k-1}
@@ -1153,6 +1178,7 @@ int eb_ctx::restore(int slot) {
     for (auto &h : snap_host)
         if (h.slot == slot) {
             steps_done = h.steps_done;
+            spikes_drained = h.spikes_drained;
             steps_since_flush = h.steps_since_flush;
         }
     CK(cudaMemsetAsync(net.rec_count, 0, sizeof(unsigned long long), stream));

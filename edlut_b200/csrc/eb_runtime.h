@@ -95,7 +95,8 @@ struct eb_ctx {
     std::vector<int64_t> in_start_host;
     std::vector<eb::PendingIn> pending;
     int64_t pending_seq = 0;
-    std::vector<double> in_times_host;
+    std::vector<double> in_times_host;   // staged input times (sorted) and their neurons
+    std::vector<uint32_t> in_cells_host;
     double *d_in_time = nullptr;
     uint32_t *d_in_cell = nullptr;
     int64_t in_total = 0, in_cap = 0;

@@ -78,6 +78,37 @@ def test_snapshot_restore_replays_identically():
     np.testing.assert_array_equal(w1, w2)
 
 
+def test_inputs_injected_after_restore_join_in_time_order():
+    """After a restore, inputs injected for the new timeline may precede inputs that
+    were staged for the abandoned one: they are merged in time order, so the run
+    equals one that had every input from the start."""
+    net, t, c, nsteps, _ = build_case("lif_rk2_stdp")
+    K, M = 600, 1400
+    sim = make_sim(net)
+    t_k = sim.step_time(K)
+    late = (np.arange(len(t)) % 2 == 1) & (t >= t_k)
+    sim.inject_spikes(t, c)
+    sim.run(M)
+    ref = spike_pairs(*sim.spikes())
+    w_ref = sim.weights()
+    sim.close()
+    sim = make_sim(net)
+    sim.inject_spikes(t[~late], c[~late])
+    sim.run(K)
+    sim.snapshot(0)
+    sim.run(M - K)  # stages the early inputs beyond step K
+    sim.restore(0)
+    sim.inject_spikes(t[late], c[late])
+    sim.run(M - K)
+    got = spike_pairs(*sim.spikes())
+    counters = sim.counters()
+    w = sim.weights()
+    sim.close()
+    np.testing.assert_array_equal(got[got[:, 0] > K], ref[ref[:, 0] > K])
+    np.testing.assert_array_equal(w, w_ref)
+    assert counters["steps"] == M
+
+
 @pytest.mark.parametrize("case", ["lif_rk2_stdp", "poisson_lif_rk2_stdp"])
 def test_reference_files_load_identically(tmp_path, case):
     """eb_load_network_files / eb_load_input_file read the reference's own text
