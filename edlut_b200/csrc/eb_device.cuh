@@ -36,6 +36,11 @@ __device__ __forceinline__ float nmda_inf(const PopDev &P, float v, float e_inh)
     return __ldg(P.nmda_table + pos);
 }
 
+// Enabled conductance types of a population (bit 0 AMPA, 1 GABA, 2 NMDA): the
+// template value when a kernel is specialised for it (EN >= 0), else P.en.
+template <int EN>
+__device__ __forceinline__ int en_mask(const PopDev &P) { return EN >= 0 ? EN : P.en; }
+
 // -------------------------------------------------------------------- LIF --
 // Refractory state of one update: the reference's derivative decides from
 // l = LastSpikeTime (ms) against tau_ref on every call; the decision only depends
@@ -65,12 +70,14 @@ __device__ __forceinline__ Refr lif_refr(const PopDev &P, int refr) {
 }
 
 // x = {V, gE, gI, gNMDA}
+template <int EN = -1>
 __device__ __forceinline__ void lif_deriv(const PopDev &P, const float *x, float *dx, Refr rf) {
     const float *p = P.p;  // e_exc e_inh e_leak v_thr c_m tau_exc tau_inh tau_ref g_leak tau_nmda
+    const int en = en_mask<EN>(P);
     float current = 0.0f;
-    if (P.en & 1) current += x[1] * (p[0] - x[0]);
-    if (P.en & 2) current += x[2] * (p[1] - x[0]);
-    if (P.en & 4) current += x[3] * nmda_inf(P, x[0], p[1]) * (p[0] - x[0]);
+    if (en & 1) current += x[1] * (p[0] - x[0]);
+    if (en & 2) current += x[2] * (p[1] - x[0]);
+    if (en & 4) current += x[3] * nmda_inf(P, x[0], p[1]) * (p[0] - x[0]);
     const float full = (current + p[8] * (p[2] - x[0])) * P.inv_c_m;
     dx[0] = rf.mode == 0 ? full : rf.mode == 1 ? rf.frac * full : 0.0f;
 }
@@ -78,22 +85,26 @@ __device__ __forceinline__ void lif_deriv(const PopDev &P, const float *x, float
 // ------------------------------------------------------------------- AdEx --
 // p = a b thr_slo_fac v_thr tau_w e_exc e_inh e_reset e_leak g_leak c_m tau_exc tau_inh tau_nmda
 // x = {V, w, gE, gI, gNMDA}
+template <int EN = -1>
 __device__ __forceinline__ void adex_deriv(const PopDev &P, const float *x, float *dx) {
     const float *p = P.p;
     const float a = p[0], slope = p[2], vthr = p[3], eexc = p[5], einh = p[6], eleak = p[8], gl = p[9];
-    if (x[0] <= vthr + 6 * slope) {
+    const int en = en_mask<EN>(P);
+    // P.adex_vmax = vthr + 6 * slope and P.adex_glslope = gl * slope: the same float
+    // operations, evaluated once on the host
+    if (x[0] <= P.adex_vmax) {
         float current = 0.0f;
-        if (P.en & 1) current += x[2] * (eexc - x[0]);
-        if (P.en & 2) current += x[3] * (einh - x[0]);
-        if (P.en & 4) current += x[4] * nmda_inf(P, x[0], einh) * (eexc - x[0]);
-        dx[0] = (gl * (eleak - x[0]) + gl * slope * expt(P, (x[0] - vthr) * P.inv_slope) - x[1] + current) * P.inv_c_m;
+        if (en & 1) current += x[2] * (eexc - x[0]);
+        if (en & 2) current += x[3] * (einh - x[0]);
+        if (en & 4) current += x[4] * nmda_inf(P, x[0], einh) * (eexc - x[0]);
+        dx[0] = (gl * (eleak - x[0]) + P.adex_glslope * expt(P, (x[0] - vthr) * P.inv_slope) - x[1] + current) * P.inv_c_m;
         dx[1] = (a * (x[0] - eleak) - x[1]) * P.inv_tau_w;
     } else if (x[0] <= 0.0f) {
         const float Vm = vthr + 6 * slope;
         float current = 0.0f;
-        if (P.en & 1) current += x[2] * (eexc - Vm);
-        if (P.en & 2) current += x[3] * (einh - Vm);
-        if (P.en & 4) current += x[4] * nmda_inf(P, Vm, einh) * (eexc - Vm);
+        if (en & 1) current += x[2] * (eexc - Vm);
+        if (en & 2) current += x[3] * (einh - Vm);
+        if (en & 4) current += x[4] * nmda_inf(P, Vm, einh) * (eexc - Vm);
         dx[0] = (gl * (eleak - Vm) + gl * slope * expt(P, (Vm - vthr) * P.inv_slope) - x[1] + current) * P.inv_c_m;
         dx[1] = (a * (x[0] - eleak) - x[1]) * P.inv_tau_w;
     } else {
@@ -106,7 +117,9 @@ __device__ __forceinline__ void adex_deriv(const PopDev &P, const float *x, floa
 // p = e_exc e_inh e_leak g_leak c_m v_thr tau_exc tau_inh tau_nmda g_na g_kd e_na e_k
 // x = {V, m, h, n, gE, gI, gNMDA}.  The clamps write the state passed in, as the
 // reference does (HHTimeDrivenModel.cpp:197-222).
+template <int EN = -1>
 __device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
+    const int en = en_mask<EN>(P);
     const float *p = P.p;
     const float eexc = p[0], einh = p[1], eleak = p[2], gl = p[3], gna = p[9], gkd = p[10], ena = p[11], ek = p[12];
     if (x[0] < ek) x[0] = ek;
@@ -123,9 +136,9 @@ __device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
     const float *r = P.hh_table + (size_t)pos * 6;
     const float am = __ldg(r + 0), bm = __ldg(r + 1), ah = __ldg(r + 2), bh = __ldg(r + 3), an = __ldg(r + 4), bn = __ldg(r + 5);
     float current = 0.0f;
-    if (P.en & 1) current += x[4] * (eexc - x[0]);
-    if (P.en & 2) current += x[5] * (einh - x[0]);
-    if (P.en & 4) current += x[6] * nmda_inf(P, x[0], einh) * (eexc - x[0]);
+    if (en & 1) current += x[4] * (eexc - x[0]);
+    if (en & 2) current += x[5] * (einh - x[0]);
+    if (en & 4) current += x[6] * nmda_inf(P, x[0], einh) * (eexc - x[0]);
     dx[0] = (current + gl * (eleak - V) + gna * m * m * m * h * (ena - V) + gkd * n * n * n * n * (ek - V)) * P.inv_c_m;
     dx[1] = (am * (1.0f - m) - bm * m);
     dx[2] = (ah * (1.0f - h) - bh * h);
@@ -135,24 +148,28 @@ __device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
 template <int KIND> struct Model;
 template <> struct Model<KIND_LIF> {
     static constexpr int ND = 1, NV = 4;
-    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr rf) { lif_deriv(P, x, dx, rf); }
+    template <int EN = -1>
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr rf) { lif_deriv<EN>(P, x, dx, rf); }
 };
 template <> struct Model<KIND_ADEX> {
     static constexpr int ND = 2, NV = 5;
-    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr) { adex_deriv(P, x, dx); }
+    template <int EN = -1>
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr) { adex_deriv<EN>(P, x, dx); }
 };
 template <> struct Model<KIND_HH> {
     static constexpr int ND = 4, NV = 7;
-    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr) { hh_deriv(P, x, dx); }
+    template <int EN = -1>
+    __device__ static void deriv(const PopDev &P, float *x, float *dx, Refr) { hh_deriv<EN>(P, x, dx); }
 };
 
 // EvaluateTimeDependentEquation: g <- 0 below 1e-9, else g * factor (enabled types only).
-template <int ND>
+template <int ND, int EN = -1>
 __device__ __forceinline__ void decay(const PopDev &P, float *x) {
     const float limit = 1e-9;
+    const int en = en_mask<EN>(P);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        if (!(P.en & (1 << c))) continue;
+        if (!(en & (1 << c))) continue;
         if (x[ND + c] < limit) x[ND + c] = 0.0f;
         else x[ND + c] *= P.decay[c];
     }
@@ -221,7 +238,7 @@ struct BdfRef {
 
 // One integration step of one neuron.  x holds all NV state variables.  Returns
 // false only if the BDF Newton matrix was singular.
-template <int KIND, int INTEG>
+template <int KIND, int INTEG, int EN = -1>
 __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, int &bdf_state, const BdfRef &H) {
     using M = Model<KIND>;
     constexpr int ND = M::ND, NV = M::NV;
@@ -229,35 +246,35 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
     float k1[NV], k2[NV], k3[NV], k4[NV], aux[NV];
     const Refr rf = (KIND == KIND_LIF) ? lif_refr(P, refr) : Refr{0, 1.0f};
     if (INTEG == INTEG_EULER) {
-        M::deriv(P, x, k1, rf);
+        M::template deriv<EN>(P, x, k1, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += dt * k1[j];
-        decay<ND>(P, x);
+        decay<ND, EN>(P, x);
     } else if (INTEG == INTEG_RK2) {
-        M::deriv(P, x, k1, rf);
+        M::template deriv<EN>(P, x, k1, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += k1[j] * dt;
-        decay<ND>(P, x);
-        M::deriv(P, x, k2, rf);
+        decay<ND, EN>(P, x);
+        M::template deriv<EN>(P, x, k2, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += (-k1[j] + k2[j]) * dt * 0.5f;
     } else if (INTEG == INTEG_RK4) {
         const float h05 = dt * 0.5f;
         const float h016 = dt * 0.166666666667f;
-        M::deriv(P, x, k1, rf);
+        M::template deriv<EN>(P, x, k1, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) aux[j] = x[j] + k1[j] * h05;
 #pragma unroll
         for (int j = ND; j < NV; ++j) aux[j] = x[j];
-        decay<ND>(P, aux);
-        M::deriv(P, aux, k2, rf);
+        decay<ND, EN>(P, aux);
+        M::template deriv<EN>(P, aux, k2, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) aux[j] = x[j] + k2[j] * h05;
-        M::deriv(P, aux, k3, rf);
+        M::template deriv<EN>(P, aux, k3, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) aux[j] = x[j] + k3[j] * dt;
-        decay<ND>(P, aux);
-        M::deriv(P, aux, k4, rf);
+        decay<ND, EN>(P, aux);
+        M::template deriv<EN>(P, aux, k4, rf);
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] += (k1[j] + 2.0f * (k2[j] + k3[j]) + k4[j]) * h016;
 #pragma unroll
@@ -266,7 +283,7 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
         int st = bdf_state;
         float pr[NV], p1[ND], c[ND], jac[ND * ND], J[ND * ND], iJ[ND * ND];
         if (st == 0) {
-            M::deriv(P, x, aux, rf);
+            M::template deriv<EN>(P, x, aux, rf);
 #pragma unroll
             for (int j = 0; j < ND; ++j) pr[j] = x[j] + dt * aux[j];
         } else {
@@ -278,7 +295,7 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
         }
 #pragma unroll
         for (int j = ND; j < NV; ++j) pr[j] = x[j];
-        decay<ND>(P, pr);
+        decay<ND, EN>(P, pr);
         const float *co = P.bdf_coef[st];
         float hist[6][ND];
         for (int q = 1; q < st; ++q)
@@ -289,7 +306,7 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
         const float eps_j = dt * 0.1f;
         const float inv_eps = 1.0f / eps_j;
         while (epsi > 1e-6 && k < 10) {
-            M::deriv(P, pr, aux, rf);
+            M::template deriv<EN>(P, pr, aux, rf);
 #pragma unroll
             for (int j = 0; j < ND; ++j) {
                 c[j] = co[0] * dt * aux[j] + co[1] * x[j];
@@ -307,7 +324,7 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
 #pragma unroll
                     for (int v = 0; v < NV; ++v) tmp[v] = pr[v];
                     tmp[j] -= eps_j;
-                    M::deriv(P, tmp, neg, rf);
+                    M::template deriv<EN>(P, tmp, neg, rf);
 #pragma unroll
                     for (int z = 0; z < ND; ++z) jac[z * ND + j] = (pos[z] - neg[z]) * inv_eps;
                 }
@@ -358,7 +375,7 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
         }
 #pragma unroll
         for (int j = 0; j < ND; ++j) x[j] = pr[j];
-        decay<ND>(P, x);
+        decay<ND, EN>(P, x);
     }
     return true;
 }

@@ -219,14 +219,14 @@ __device__ __forceinline__ void store_aux(const PopDev &P, int64_t i, const Neur
 
 // Advance one neuron (after its arrivals were folded); returns spike flag.  The
 // integer state is updated in ax (store_aux writes it back).
-template <int KIND, int INTEG>
+template <int KIND, int INTEG, int EN = -1>
 __device__ __forceinline__ bool advance_neuron(const PopDev &P, const NetDev &N, int64_t i, float *x, NeuronAux &ax) {
     constexpr int NV = Model<KIND>::NV;
     int refr = ax.refr;
     int bst = ax.bst;
     BdfRef H{P.bdf_D, P.bdf_P, P.n, i};
     const float prevV = x[0];
-    if (!integrate<KIND, INTEG>(P, x, refr, bst, H)) atomicOr(N.flags, FLAG_BDF_SINGULAR);
+    if (!integrate<KIND, INTEG, EN>(P, x, refr, bst, H)) atomicOr(N.flags, FLAG_BDF_SINGULAR);
     if (KIND == KIND_LIF && refr >= 0) refr++;  // AddElapsedTime
     bool reset = false;
     const bool sp = spike_condition<KIND>(P, x, prevV, reset);
@@ -363,7 +363,7 @@ constexpr int kNarrowTile = 256;
 
 // One step of neuron i (lanes with active unset only join the warp collectives);
 // x and ax hold its state, loaded and stored by the caller.
-template <int KIND, int INTEG>
+template <int KIND, int INTEG, int EN = -1>
 __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, int64_t k, int64_t i, bool active,
                                             float *x, NeuronAux &ax, bool list, double push_inv_dt) {
     constexpr int ND = Model<KIND>::ND;
@@ -400,7 +400,7 @@ __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, in
                 for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
             }
         }
-        sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax);
+        sp = advance_neuron<KIND, INTEG, EN>(P, N, i, x, ax);
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
         if (sp && P.post_t) note_post_spike(P, N, i, k);
     }
@@ -440,9 +440,16 @@ __device__ __forceinline__ void update_narrow_tile(const PopDev &P, const NetDev
 // HH under BDF holds the Newton state (Jacobian, inverse, history) in about 120
 // registers, which leaves 2 blocks per SM; bounded to 3 blocks (80 registers, a
 // 44-byte spill) a 100k-neuron population fits one wave and its steps take a
-// quarter less time.  Every other instantiation keeps the compiler's choice.
-template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kNarrowTile, (KIND == KIND_HH && INTEG == INTEG_BDF) ? 3 : 0) k_update_narrow(PopDev P, NetDev N, int rel, int nsteps,
+// quarter less time.  LIF and AdEx under the explicit methods are bounded to 6
+// blocks (40 registers, spills of 8-12 bytes): a fifth more resident neurons than
+// at the compiler's 48, so a 250k-neuron population takes 1.06 waves, not 1.32.
+// EN >= 0: the population's enabled conductance types fixed at compile time.
+constexpr int narrow_min_blocks(int kind, int integ) {
+    return (kind == KIND_HH && integ == INTEG_BDF) ? 3 : (kind != KIND_HH && integ != INTEG_BDF) ? 6 : 0;
+}
+
+template <int KIND, int INTEG, int EN>
+__global__ void __launch_bounds__(kNarrowTile, narrow_min_blocks(KIND, INTEG)) k_update_narrow(PopDev P, NetDev N, int rel, int nsteps,
                                                                 double push_inv_dt) {
     const int64_t k = cur_step(N, rel);
     const bool list = nsteps == 1;
@@ -455,7 +462,7 @@ __global__ void __launch_bounds__(kNarrowTile, (KIND == KIND_HH && INTEG == INTE
         load_state<KIND>(P, i, x);
         ax = load_aux<KIND, INTEG>(P, i);
     }
-    for (int s = 0; s < nsteps; ++s) narrow_step<KIND, INTEG>(P, N, k + s, i, active, x, ax, list, push_inv_dt);
+    for (int s = 0; s < nsteps; ++s) narrow_step<KIND, INTEG, EN>(P, N, k + s, i, active, x, ax, list, push_inv_dt);
     if (active) {
         store_state<KIND>(P, i, x);
         store_aux<KIND, INTEG>(P, i, ax);
@@ -875,13 +882,17 @@ __global__ void __launch_bounds__(256) k_push(PopDev P, NetDev N, int rel, doubl
     for (int64_t s = blockIdx.x; s < ns; s += gridDim.x) push_spike(P, N, k, s, inv_dt);
 }
 
-// Input spikes of steps k .. k+nsteps-1 (their deliveries are independent).
+// Input spikes of steps k .. k+nsteps-1.  Their deliveries are independent, so the
+// window's inputs -- one contiguous range of the staged list -- are spread over
+// the blocks at once; each block finds its spike's step among the window's
+// input ranges.
 __global__ void __launch_bounds__(256) k_input_push(NetDev N, int rel, int nsteps, double inv_dt) {
     const int64_t k0 = cur_step(N, rel);
-    for (int s = 0; s < nsteps; ++s) {
-        const int64_t k = k0 + s;
-        const int64_t q0 = N.in_start[k], q1 = N.in_start[k + 1];
-        for (int64_t q = q0 + blockIdx.x; q < q1; q += gridDim.x) input_spike(N, k, q, inv_dt);
+    const int64_t q0 = N.in_start[k0], q1 = N.in_start[k0 + nsteps];
+    for (int64_t q = q0 + blockIdx.x; q < q1; q += gridDim.x) {
+        int64_t k = k0;
+        while (k + 1 < k0 + nsteps && N.in_start[k + 1] <= q) ++k;
+        input_spike(N, k, q, inv_dt);
     }
 }
 
@@ -1155,8 +1166,11 @@ static void launch_update_t(const PopDev &P, const NetDev &N, int rel, int nstep
         const int blocks = (int)std::min<int64_t>(P.n, 148 * 8);
         k_update_wide<KIND, INTEG><<<blocks, kWideThreads, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
     } else {
+        // the common conductance sets get kernels with the set compiled in
         const int blocks = (int)((P.n + 255) / 256);
-        k_update_narrow<KIND, INTEG><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        if (P.en == 1) k_update_narrow<KIND, INTEG, 1><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        else if (P.en == 3) k_update_narrow<KIND, INTEG, 3><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        else k_update_narrow<KIND, INTEG, -1><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
     }
 }
 

@@ -389,6 +389,8 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
                 D.inv_c_m = inv_double(pr[10]);
                 D.inv_slope = inv_double(pr[2]);
                 D.inv_tau_w = inv_double(pr[4]);
+                D.adex_vmax = pr[3] + 6 * pr[2];
+                D.adex_glslope = pr[9] * pr[2];
                 tau[0] = pr[11]; tau[1] = pr[12]; tau[2] = pr[13];
                 init[0] = pr[8];
                 nmda = make_nmda_table(pr[5], pr[6], &D.nmda_aux);

@@ -64,6 +64,7 @@ struct PopDev {
     float p[16];     // model parameters in .cfg order
     float dt_s, dt_ms;
     float inv_c_m, inv_slope, inv_tau_w;
+    float adex_vmax, adex_glslope;  // AdEx: vthr + 6 * slope, gl * slope
     float decay[3];  // conductance decay factor per step (RK4: per half step)
     float bdf_coef[7][7];
     float init[kMaxVars];
