@@ -44,9 +44,9 @@ __device__ __forceinline__ float expt_net(const NetDev &N, float v) {
     return 0.0f;
 }
 
-// STDPWeightChange::ApplyPreSynapticSpike on synapse tp at arrival time a.
-// The record r is the synapse's state as loaded; the updated fields are stored.
-__device__ __forceinline__ void stdp_pre(const NetDev &N, uint32_t tp, const SynRec &r, double a) {
+// STDPWeightChange::ApplyPreSynapticSpike on the record r of a synapse at arrival
+// time a (src/learning_rules/STDPWeightChange.cpp:43-56), in place.
+__device__ __forceinline__ void stdp_pre_rec(const NetDev &N, SynRec &r, double a) {
     const float *rp = N.rule_par + r.rule * 6;
     float el = (float)(a - r.last);
     float pre = r.pre * expt_net(N, -el * rp[4]);
@@ -56,11 +56,21 @@ __device__ __forceinline__ void stdp_pre(const NetDev &N, uint32_t tp, const Syn
     w += -rp[2] * post;
     const float mw = r.maxw;
     if (w > mw) w = mw; else if (w < 0.0f) w = 0.0f;
+    r.w = w;
+    r.pre = pre;
+    r.post = post;
+    r.last = a;
+}
+
+// The same on synapse tp: r is its state as loaded; the updated fields are stored.
+__device__ __forceinline__ void stdp_pre(const NetDev &N, uint32_t tp, const SynRec &r, double a) {
+    SynRec u = r;
+    stdp_pre_rec(N, u, a);
     SynRec *s = N.syn + tp;
-    s->w = w;
-    s->pre = pre;
-    s->post = post;
-    s->last = a;
+    s->w = u.w;
+    s->pre = u.pre;
+    s->post = u.post;
+    s->last = u.last;
 }
 
 // STDPWeightChange::ApplyPostSynapticSpike on a synapse record for a spike of its
@@ -488,12 +498,19 @@ constexpr int kWideSmem = 1024;
 constexpr int kRankSort = 256;
 static_assert(kRankSort <= kWideThreads && kWideThreads == kNarrowTile, "wide blocks rank with one thread per arrival");
 
+// Steps of one launch (the runtime's window length).
+constexpr int kMaxWindow = 8;
+
 struct WideSmem {
     int spiked;                         // the block's neuron spiked this step (fused fan-out)
     int ring_ok;                        // ring, ring_f and ring_n hold the neuron's ring
     uint32_t ring_n;                    // post-synaptic spikes noted so far (deferred STDP)
     uint32_t next_c;                    // next step's arrival count (copied ahead)
     float g[3];                         // conductances handed to the per-type adders
+    uint32_t wcnt[kMaxWindow];          // staged window: arrivals of each step
+    uint32_t woff[kMaxWindow + 1];      // and their offsets (exclusive scan)
+    int dup;                            // a synapse of the staged chunk delivers twice
+    int next_s;                         // first step of the chunk's next round
     unsigned long long khi[kRankSort];  // arrival time keys
     uint32_t klo[kRankSort];            // synapse order
     uint32_t rank[kRankSort];           // delivery position
@@ -782,11 +799,301 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
     }
 }
 
-// Steps k .. k+nsteps-1 of the block's neurons (spike list as in k_update_narrow).
+// ------------------------------------------------------ staged wide window --
+// A launch's window of steps for one wide neuron with every delivery of the
+// window taken in at once.  All buckets of the window's steps are final when the
+// launch starts, so the block stages the arrivals of as many consecutive steps as
+// fit in shared memory (a chunk) and every arrival's delivery position within its
+// step, in parallel: a few dependent global round trips per chunk instead of per
+// step.  When every synapse of the chunk delivers once (the usual case), the
+// chunk's steps run in rounds: the whole block computes, in parallel, every
+// remaining arrival's synapse update -- deferred post-synaptic catch-up on the
+// target's spikes so far, the delivered weight at its position, the STDP pre
+// update -- then warp 0 runs the steps in order (ordered sums, integration, spike,
+// fan-out) until the neuron spikes.  A spike changes the catch-up of the later
+// arrivals, so the next round recomputes those from their records in global
+// memory, untouched until the chunk writes back.  A chunk in which a synapse
+// delivers on two steps runs its steps serially on warp 0 over one staged record
+// per synapse; a step with more arrivals than the stage holds runs on the
+// per-step path (wide_step).
+constexpr int kStage = 1024;          // arrivals of one chunk
+constexpr int kStageHashBits = 11;    // open-addressing table of the chunk's synapses
+constexpr int kStageHash = 1 << kStageHashBits;
+constexpr uint32_t kHashEmpty = 0xffffffffu;
+static_assert(kStage <= kWideSmem, "a staged chunk's weights fit the fold buffer");
+
+struct StageSmem {
+    Arrival arr[kStage];               // the chunk's arrivals, step by step in bucket order
+    SynRec rec[kStage];                // updated synapse records (serial path: at the owning arrival)
+    unsigned long long key[kStage];    // order-preserving integer key of each arrival time
+    uint32_t hkey[kStageHash];         // tpos of the synapse claiming a slot
+    uint16_t hval[kStageHash];         // its owning arrival
+    uint16_t own[kStage];              // per arrival: the arrival whose staged record it uses
+    uint16_t rank[kStage];             // per arrival: delivery position within its step
+};
+
+__host__ __device__ constexpr size_t stage_smem_bytes() { return sizeof(StageSmem); }
+
+__device__ __forceinline__ int stage_step_of(const WideSmem &S, int s0, uint32_t g) {
+    int s = s0;
+    while (S.woff[s + 1] <= g) ++s;
+    return s;
+}
+
+// Sum of the c weights sw[o0..o0+c) onto g in order, loads issued 8 at a time.
+__device__ __forceinline__ float ordered_sum1(const WideSmem &S, uint32_t o0, uint32_t c, float g) {
+    uint32_t q = 0;
+    for (; q + 8 <= c; q += 8) {
+        float w[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) w[u] = S.sw[o0 + q + u];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) g += w[u];
+    }
+    for (; q < c; ++q) g += S.sw[o0 + q];
+    return g;
+}
+
+// Add the c weights sw[o0..o0+c) (types sty[]) to the conductances x[ND..ND+2] in
+// order: each conductance sees its own type's weights in delivery order, as the
+// reference's successive additions.  A population with one enabled conductance
+// receives weights of that type only.
+template <int ND>
+__device__ __forceinline__ void ordered_sum(const WideSmem &S, uint32_t o0, uint32_t c, float *x, int en) {
+    if (en == 1) { x[ND] = ordered_sum1(S, o0, c, x[ND]); return; }
+    if (en == 2) { x[ND + 1] = ordered_sum1(S, o0, c, x[ND + 1]); return; }
+    if (en == 4) { x[ND + 2] = ordered_sum1(S, o0, c, x[ND + 2]); return; }
+    float g0 = x[ND], g1 = x[ND + 1], g2 = x[ND + 2];
+    uint32_t q = 0;
+    for (; q + 8 <= c; q += 8) {
+        float w[8];
+        int t[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) { w[u] = S.sw[o0 + q + u]; t[u] = S.sty[o0 + q + u]; }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (t[u] == 0) g0 += w[u];
+            else if (t[u] == 1) g1 += w[u];
+            else g2 += w[u];
+        }
+    }
+    for (; q < c; ++q) {
+        const int t = S.sty[o0 + q];
+        const float w = S.sw[o0 + q];
+        if (t == 0) g0 += w;
+        else if (t == 1) g1 += w;
+        else g2 += w;
+    }
+    x[ND] = g0;
+    x[ND + 1] = g1;
+    x[ND + 2] = g2;
+}
+
+// Lane 0 of warp 0, after step ks's conductances are in x: integrate, test the
+// spike, note it for deferred post-synaptic STDP (global ring and its staged
+// copy), trace, spike list and recording.  Returns the spike flag.
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
-                                                              double push_inv_dt) {
+__device__ __forceinline__ int wide_advance(const PopDev &P, const NetDev &N, int64_t ks, int64_t i, WideSmem &S,
+                                            float *x, NeuronAux &ax, bool list, bool ring) {
+    const int64_t gi = P.first + i;
+    const int sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax) ? 1 : 0;
+    if (sp && ring) {
+        note_post_spike(P, N, i, ks);
+        const uint32_t n1 = P.post_n[i], q = (n1 - 1) % kPostRing;
+        S.ring_n = n1;
+        S.ring[q] = P.post_t[i * kPostRing + q];
+        if (P.post_f) S.ring_f[q] = P.post_f[i * kPostRing + q];
+    }
+    record_trace(P, N, ks, gi, x, Model<KIND>::NV);
+    if (sp) {
+        if (list) {
+            const uint32_t o = atomicAdd(&P.spk_count[ks & 1], 1u);
+            if (o < (uint32_t)P.n) P.spk[o] = (uint32_t)i;
+            else atomicOr(N.flags, FLAG_SPIKELIST_OVERFLOW);
+        }
+        if (N.rec_buf) {
+            const unsigned long long ro = atomicAdd(N.rec_count, 1ull);
+            if (ro < (unsigned long long)N.rec_cap)
+                N.rec_buf[ro] = ((unsigned long long)ks << 32) | (unsigned long long)gi;
+            else atomicOr(N.flags, FLAG_RECORD_OVERFLOW);
+        }
+    }
+    return sp;
+}
+
+template <int KIND, int INTEG>
+__device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
+                                            StageSmem &G, float *x, NeuronAux &ax, int nsteps, bool list,
+                                            double push_inv_dt) {
+    constexpr int ND = Model<KIND>::ND;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31;
+    const int64_t gi = P.first + i;
+    const uint32_t capg = N.cap[gi];
+    const int64_t rbase = N.cap_base[gi];
+    const bool ring = P.post_t != nullptr;
+    const int prule = P.post_f ? P.post_rule : -1;
+    if (tid < nsteps) {
+        uint32_t c = N.cnt[(int64_t)((k + tid) & (N.R - 1)) * N.n_neurons + gi];
+        if (c > capg) { atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
+        S.wcnt[tid] = c;
+    }
+    if (ring && !S.ring_ok) {
+        for (int q = tid; q < kPostRing; q += nt) {
+            S.ring[q] = P.post_t[i * kPostRing + q];
+            if (P.post_f) S.ring_f[q] = P.post_f[i * kPostRing + q];
+        }
+        if (tid == nt - 1) S.ring_n = P.post_n[i];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        S.woff[0] = 0;
+        for (int s = 0; s < nsteps; ++s) S.woff[s + 1] = S.woff[s] + S.wcnt[s];
+        if (ring) S.ring_ok = 1;
+    }
+    __syncthreads();
+    int s0 = 0;
+    while (s0 < nsteps) {
+        int s1 = s0;
+        while (s1 < nsteps && S.woff[s1 + 1] - S.woff[s0] <= (uint32_t)kStage) ++s1;
+        if (s1 == s0) {  // this step alone overflows the stage
+            int pf_n = 0;
+            wide_step<KIND, INTEG>(P, N, k + s0, i, S, x, ax, list, push_inv_dt, pf_n, false);
+            __syncthreads();
+            ++s0;
+            continue;
+        }
+        const uint32_t a0 = S.woff[s0], T = S.woff[s1] - a0;
+        for (uint32_t a = tid; a < T; a += nt) {
+            const int s = stage_step_of(S, s0, a0 + a);
+            const int slot = (int)((k + s) & (N.R - 1));
+            const Arrival v = N.rec[(int64_t)slot * N.cap_total + rbase + (a0 + a - S.woff[s])];
+            G.arr[a] = v;
+            G.key[a] = time_key(v.a);
+        }
+        for (int h = tid; h < kStageHash; h += nt) G.hkey[h] = kHashEmpty;
+        if (tid == 0) S.dup = 0;
+        __syncthreads();
+        if (tid >= s0 && tid < s1) N.cnt[(int64_t)((k + tid) & (N.R - 1)) * N.n_neurons + gi] = 0;
+        if (tid == 0 && T) atomicAdd(P.events, (unsigned long long)T);
+        // synapses of the chunk: the arrival that claims a synapse's slot owns it
+        for (uint32_t a = tid; a < T; a += nt) {
+            const uint32_t tp = G.arr[a].tpos;
+            uint32_t h = (tp * 2654435761u) >> (32 - kStageHashBits);
+            for (;;) {
+                const uint32_t prev = atomicCAS(&G.hkey[h], kHashEmpty, tp);
+                if (prev == kHashEmpty) { G.hval[h] = (uint16_t)a; break; }
+                if (prev == tp) { S.dup = 1; break; }
+                h = (h + 1) & (kStageHash - 1);
+            }
+            G.own[a] = (uint16_t)h;
+        }
+        __syncthreads();
+        const bool dup = S.dup != 0;
+        for (uint32_t a = tid; a < T; a += nt) {
+            const uint32_t o = G.hval[G.own[a]];
+            G.own[a] = (uint16_t)o;
+            if (dup && o == a) {  // serial path: one staged record per synapse, caught up to the chunk
+                SynRec r = N.syn[G.arr[a].tpos];
+                if (r.rule >= 0 && ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, prule, r);
+                G.rec[a] = r;
+            }
+            // delivery position: arrivals of the same step before it in (time,
+            // synapse order) order -- a step's synapses are distinct here -- on the
+            // integer keys of the times
+            const int s = stage_step_of(S, s0, a0 + a);
+            const uint32_t b0 = S.woff[s] - a0, b1 = S.woff[s + 1] - a0;
+            const unsigned long long ka = G.key[a];
+            const uint32_t pa = G.arr[a].spos;
+            uint32_t r = 0;
+#pragma unroll 4
+            for (uint32_t b = b0; b < b1; ++b) {
+                const unsigned long long kb = G.key[b];
+                r += (kb < ka || (kb == ka && G.arr[b].spos < pa)) ? 1u : 0u;
+            }
+            G.rank[a] = (uint16_t)r;
+        }
+        __syncthreads();
+        if (!dup) {
+            int s = s0;
+            while (s < s1) {
+                for (uint32_t a = S.woff[s] - a0 + tid; a < T; a += nt) {
+                    SynRec r = N.syn[G.arr[a].tpos];
+                    if (r.rule >= 0 && ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, prule, r);
+                    const uint32_t pos = S.woff[stage_step_of(S, s0, a0 + a)] - a0 + G.rank[a];
+                    S.sw[pos] = r.w;
+                    S.sty[pos] = r.stype;
+                    if (r.rule >= 0) stdp_pre_rec(N, r, G.arr[a].a);
+                    G.rec[a] = r;
+                }
+                __syncthreads();
+                if (tid < 32) {
+                    int next = s1;
+                    for (int j = s; j < s1; ++j) {
+                        int sp = 0;
+                        if (lane == 0) {
+                            ordered_sum<ND>(S, S.woff[j] - a0, S.wcnt[j], x, P.en);
+                            sp = wide_advance<KIND, INTEG>(P, N, k + j, i, S, x, ax, list, ring);
+                        }
+                        sp = __shfl_sync(0xffffffffu, sp, 0);
+                        if (sp && push_inv_dt > 0.0) push_from(P, N, k + j, gi, lane, 32, push_inv_dt);
+                        if (sp && ring) { next = j + 1; break; }
+                    }
+                    if (lane == 0) S.next_s = next;
+                }
+                __syncthreads();
+                s = S.next_s;
+            }
+        } else if (tid < 32) {
+            for (int s = s0; s < s1; ++s) {
+                const int64_t ks = k + s;
+                const uint32_t o0 = S.woff[s] - a0, c = S.wcnt[s];
+                for (uint32_t a = o0 + lane; a < o0 + c; a += 32) {
+                    SynRec &sr = G.rec[G.own[a]];
+                    SynRec r = sr;
+                    if (r.rule >= 0 && ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, prule, r);
+                    S.sw[o0 + G.rank[a]] = r.w;
+                    S.sty[o0 + G.rank[a]] = r.stype;
+                    if (r.rule >= 0) {
+                        stdp_pre_rec(N, r, G.arr[a].a);
+                        sr = r;
+                    }
+                }
+                __syncwarp();
+                int sp = 0;
+                if (lane == 0) {
+                    ordered_sum<ND>(S, o0, c, x, P.en);
+                    sp = wide_advance<KIND, INTEG>(P, N, ks, i, S, x, ax, list, ring);
+                }
+                sp = __shfl_sync(0xffffffffu, sp, 0);
+                if (sp && push_inv_dt > 0.0) push_from(P, N, ks, gi, lane, 32, push_inv_dt);
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        for (uint32_t a = tid; a < T; a += nt) {
+            if (G.own[a] != a || G.rec[a].rule < 0) continue;
+            const SynRec &r = G.rec[a];
+            SynRec *d = N.syn + G.arr[a].tpos;
+            d->w = r.w;
+            d->pre = r.pre;
+            d->post = r.post;
+            d->last = r.last;
+        }
+        __syncthreads();
+        s0 = s1;
+    }
+}
+
+// Steps k .. k+nsteps-1 of the block's neurons (spike list as in k_update_narrow).
+// Populations whose synapses cannot deliver twice in one step take the staged
+// window; the others run step by step.  Two blocks per SM (the staging area allows
+// two): up to 128 registers, so the serial per-step code runs without spills.
+template <int KIND, int INTEG>
+__global__ void __launch_bounds__(kWideThreads, 2) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
+                                                                 double push_inv_dt) {
     __shared__ WideSmem S;
+    extern __shared__ __align__(32) unsigned char stage_raw[];
+    StageSmem &G = *reinterpret_cast<StageSmem *>(stage_raw);
     const int64_t k = cur_step(N, rel);
     const bool list = nsteps == 1;
     if (list && blockIdx.x == 0 && threadIdx.x == 0) P.spk_count[(k + 1) & 1] = 0;
@@ -798,13 +1105,19 @@ __global__ void __launch_bounds__(kWideThreads) k_update_wide(PopDev P, NetDev N
             ax = load_aux<KIND, INTEG>(P, i);
             S.ring_ok = 0;
         }
-        int pf_n = 0;
-        for (int s = 0; s < nsteps; ++s)
-            wide_step<KIND, INTEG>(P, N, k + s, i, S, x, ax, list, push_inv_dt, pf_n, s + 1 < nsteps);
+        __syncthreads();  // S.ring_ok reset before any thread reads it
+        if (!P.may_repeat && nsteps <= kMaxWindow) {
+            wide_window<KIND, INTEG>(P, N, k, i, S, G, x, ax, nsteps, list, push_inv_dt);
+        } else {
+            int pf_n = 0;
+            for (int s = 0; s < nsteps; ++s)
+                wide_step<KIND, INTEG>(P, N, k + s, i, S, x, ax, list, push_inv_dt, pf_n, s + 1 < nsteps);
+        }
         if (threadIdx.x == 0) {
             store_state<KIND>(P, i, x);
             store_aux<KIND, INTEG>(P, i, ax);
         }
+        __syncthreads();  // the next neuron's staging reuses S
     }
 }
 
@@ -1164,7 +1477,7 @@ template <int KIND, int INTEG>
 static void launch_update_t(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st) {
     if (P.wide) {
         const int blocks = (int)std::min<int64_t>(P.n, 148 * 8);
-        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, stage_smem_bytes(), st>>>(P, N, rel, nsteps, push_inv_dt);
     } else {
         // the common conductance sets get kernels with the set compiled in
         const int blocks = (int)((P.n + 255) / 256);
@@ -1182,6 +1495,25 @@ static void launch_update_k(const PopDev &P, const NetDev &N, int rel, int nstep
     case INTEG_RK4: launch_update_t<KIND, INTEG_RK4>(P, N, rel, nsteps, push_inv_dt, st); break;
     default: launch_update_t<KIND, INTEG_BDF>(P, N, rel, nsteps, push_inv_dt, st); break;
     }
+}
+
+template <int KIND>
+static cudaError_t prepare_wide_k() {
+    const int bytes = (int)stage_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
+}
+
+// Opt the wide updates into their staging area (dynamic shared memory above the
+// 48 KB default) on the current device; once per device, before any launch.
+cudaError_t prepare_update_kernels() {
+    cudaError_t e = prepare_wide_k<KIND_LIF>();
+    if (e == cudaSuccess) e = prepare_wide_k<KIND_ADEX>();
+    if (e == cudaSuccess) e = prepare_wide_k<KIND_HH>();
+    return e;
 }
 
 void launch_update(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st) {

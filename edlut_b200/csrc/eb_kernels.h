@@ -9,6 +9,8 @@ namespace eb {
 // population spike list is not kept (the eager post-synaptic and separate fan-out
 // kernels cannot follow such a launch).
 void launch_update(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st);
+// Kernel attributes the update launches need (once per device, before launching).
+cudaError_t prepare_update_kernels();
 constexpr int kPostThreads = 256;  // plastic synapses per post-STDP work item
 void launch_push(const PopDev &P, const NetDev &N, int rel, double inv_dt, int blocks, int threads, cudaStream_t st);
 void launch_input_push(const NetDev &N, int rel, int nsteps, double inv_dt, int blocks, int threads, cudaStream_t st);

@@ -531,6 +531,7 @@ int eb_ctx::finalize(int64_t *out_sorted_perm) {
         join_ev.push_back(b);
     }
     if ((rc = setup_persistent())) return rc;
+    CK(prepare_update_kernels());
     CK(cudaStreamSynchronize(st));
     finalized = true;
     steps_done = 0;
