@@ -38,6 +38,10 @@ SIGNATURES = [
                                             c_f32p, c_f32p, c_i32p]),
     ("eb_set_bucket_limit", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32]),
     ("eb_set_wide_indegree", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64]),
+    ("eb_set_barrier_wait", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]),
+    ("eb_enable_conductances", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("eb_population_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
     ("eb_finalize", ctypes.c_int, [ctypes.c_void_p, c_i64p]),
     ("eb_load_network_files", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p]),
     ("eb_inject_spikes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, c_f32p, c_i64p]),

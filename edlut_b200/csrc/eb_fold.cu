@@ -90,8 +90,47 @@ __global__ void k_fold_scatter(int64_t n, const int32_t *target, const double *t
     }
 }
 
-// One thread per target: insertion-sort its arrivals by (time, index) in place,
-// then add the weights in that order.
+// Restore the heap property below node j of the max-heap r[0..c) by (time, index).
+__device__ __forceinline__ void sift_down(FoldRec *r, uint32_t j, uint32_t c) {
+    const FoldRec v = r[j];
+    for (;;) {
+        uint32_t ch = 2 * j + 1;
+        if (ch >= c) break;
+        if (ch + 1 < c && fold_less(r[ch], r[ch + 1])) ++ch;
+        if (!fold_less(v, r[ch])) break;
+        r[j] = r[ch];
+        j = ch;
+    }
+    r[j] = v;
+}
+
+// Sort r[0..c) by (time, index) in place: insertion sort for the few arrivals a
+// target usually gets, heapsort (O(c log c), no extra memory) beyond, so a batch
+// that sends every arrival to one target stays bounded.  The keys are distinct
+// (the index), so both give the same order.
+constexpr uint32_t kFoldInsertionMax = 32;
+
+__device__ __forceinline__ void fold_sort(FoldRec *r, uint32_t c) {
+    if (c <= kFoldInsertionMax) {
+        for (uint32_t a = 1; a < c; ++a) {
+            FoldRec v = r[a];
+            int b = (int)a - 1;
+            while (b >= 0 && fold_less(v, r[b])) { r[b + 1] = r[b]; --b; }
+            r[b + 1] = v;
+        }
+        return;
+    }
+    for (uint32_t j = c / 2; j-- > 0;) sift_down(r, j, c);
+    for (uint32_t e = c - 1; e > 0; --e) {
+        const FoldRec top = r[0];
+        r[0] = r[e];
+        r[e] = top;
+        sift_down(r, 0, e);
+    }
+}
+
+// One thread per target: sort its arrivals by (time, index) in place, then add
+// the weights in that order.
 __global__ void k_fold_apply(int64_t m, const uint32_t *cnt, const uint32_t *offs, FoldRec *rec,
                              const int8_t *type, const float *weight, float *g_exc, float *g_inh, float *g_nmda) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -99,12 +138,7 @@ __global__ void k_fold_apply(int64_t m, const uint32_t *cnt, const uint32_t *off
     const uint32_t c = cnt[t];
     if (!c) return;
     FoldRec *r = rec + offs[t];
-    for (uint32_t a = 1; a < c; ++a) {
-        FoldRec v = r[a];
-        int b = (int)a - 1;
-        while (b >= 0 && fold_less(v, r[b])) { r[b + 1] = r[b]; --b; }
-        r[b + 1] = v;
-    }
+    fold_sort(r, c);
     float ge = g_exc ? g_exc[t] : 0.0f, gi = g_inh ? g_inh[t] : 0.0f, gn = g_nmda ? g_nmda[t] : 0.0f;
     for (uint32_t a = 0; a < c; ++a) {
         const uint32_t i = r[a].i;

@@ -1227,8 +1227,7 @@ __global__ void __launch_bounds__(256) k_post_stdp(PopDev P, NetDev N, int rel, 
 // separated by grid barriers.  Removes the per-launch cost (about 3 us per
 // kernel on this part) and the graph dependency latency of the K x (2..3)
 // launches it replaces.  Every barrier wait is bounded: on timeout the block
-// records FLAG_BARRIER_TIMEOUT and the kernel ends.
-constexpr unsigned long long kBarrierSpinLimit = 1ull << 24;
+// records FLAG_BARRIER_TIMEOUT and the kernel ends (I.spin_limit polls).
 constexpr int kTlSlots = 6;
 constexpr int kBarrierGroup = 16;     // blocks per first-level counter
 constexpr int kBarrierStride = 32;    // words between counters (own 128-byte line)
@@ -1239,7 +1238,10 @@ constexpr int kBarrierStride = 32;    // words between counters (own 128-byte li
 // polls.  Spreads the arrival atomics over many cache lines instead of
 // serialising gridDim.x of them on one.  Layout of bar (words):
 //   [0] generation, [kBarrierStride] root count, [(g+2)*kBarrierStride] group g.
-__device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned nblocks, uint32_t *flags) {
+// I.withhold: block 0 does not arrive, so every block's wait runs out -- the
+// failure path, exercised on purpose with a short I.spin_limit.
+__device__ __forceinline__ bool grid_sync(const PersistInfo &I, unsigned nblocks, uint32_t *flags) {
+    unsigned *bar = I.bar;
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1253,7 +1255,8 @@ __device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned nblocks, uint3
         unsigned *root = bar + kBarrierStride;
         __threadfence();
         bool last = false;
-        if (atomicAdd(gc, 1u) == in_grp - 1) {
+        if (I.withhold && blockIdx.x == 0) {
+        } else if (atomicAdd(gc, 1u) == in_grp - 1) {
             *gc = 0;
             __threadfence();
             if (atomicAdd(root, 1u) == ngroups - 1) {
@@ -1268,7 +1271,7 @@ __device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned nblocks, uint3
             unsigned long long spins = 0;
             while (*gen == g) {
                 __nanosleep(32);
-                if (++spins > kBarrierSpinLimit) {
+                if (++spins > I.spin_limit) {
                     atomicOr(flags, FLAG_BARRIER_TIMEOUT);
                     s_ok = 0;
                     break;
@@ -1299,7 +1302,7 @@ __device__ __forceinline__ void update_item_k(const PopDev &P, const NetDev &N, 
     case INTEG_RK4: update_item<KIND, INTEG_RK4>(P, N, k, local, S); break;
     default:
         if constexpr (CLASS >= 2) update_item<KIND, INTEG_BDF>(P, N, k, local, S);
-        else if (threadIdx.x == 0) atomicOr(N.flags, FLAG_BARRIER_TIMEOUT);
+        else if (threadIdx.x == 0) atomicOr(N.flags, FLAG_PERSIST_UNSUPPORTED);
         break;
     }
 }
@@ -1388,7 +1391,7 @@ __global__ void __launch_bounds__(kNarrowTile, CLASS == 0 ? 3 : (CLASS == 1 ? 2 
         if (I.has_inputs) { q0 = N.in_start[k]; n_in = N.in_start[k + 1] - q0; }
         if (I.has_inputs && !I.inputs_concurrent) {
             for (int64_t it = blockIdx.x; it < n_in; it += nb) input_spike(N, k, q0 + it, I.inv_dt);
-            if (!grid_sync(I.bar, nb, N.flags)) return;
+            if (!grid_sync(I, nb, N.flags)) return;
             n_in = 0;
         }
         // phase A: longest items first -- the populations in I.order (wide ones
@@ -1425,7 +1428,7 @@ __global__ void __launch_bounds__(kNarrowTile, CLASS == 0 ? 3 : (CLASS == 1 ? 2 
         }
         tl_mark(I, r, 1);
         tl_put(I, r, 5, (unsigned long long)n_items);
-        if (!grid_sync(I.bar, nb, N.flags)) return;
+        if (!grid_sync(I, nb, N.flags)) return;
         tl_mark(I, r, 2);
         // phase B
         int64_t cnt[kMaxPersistPops];
@@ -1447,7 +1450,7 @@ __global__ void __launch_bounds__(kNarrowTile, CLASS == 0 ? 3 : (CLASS == 1 ? 2 
             else push_spike(P, N, k, local - np, I.inv_dt);
         }
         tl_mark(I, r, 3);
-        if (!grid_sync(I.bar, nb, N.flags)) return;
+        if (!grid_sync(I, nb, N.flags)) return;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *const_cast<int64_t *>(N.step) += K;
 }

@@ -34,7 +34,10 @@ struct PersistInfo {
     unsigned long long *queue;        // item counters [step parity][phase], 128 bytes apart
     unsigned long long *tl;           // optional timeline [tl_steps][4][grid] (globaltimer ns)
     int tl_steps;
+    unsigned long long spin_limit;    // polls of a grid-barrier wait before it reports a timeout
+    int withhold;                     // block 0 does not arrive at barriers (exercises the timeout)
 };
+constexpr unsigned long long kBarrierSpinLimit = 1ull << 24;
 int persist_class_of(int kind, int integ);
 int persistent_blocks_per_sm(int cls);
 cudaError_t launch_persistent(int cls, const PopDev *pops, const PersistInfo &I, const NetDev &N, int K, int grid,

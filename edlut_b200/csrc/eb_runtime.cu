@@ -833,6 +833,8 @@ int eb_ctx::setup_persistent() {
     int n_model = 0;
     persist_class = 0;
     memset(&pinfo, 0, sizeof(pinfo));
+    pinfo.spin_limit = barrier_spin_limit;
+    pinfo.withhold = barrier_withhold ? 1 : 0;
     for (auto &p : pops) {
         if (p.kind == KIND_INPUT) continue;
         if (p.kind == KIND_POISSON) return EB_OK;  // generators run on the graph path only
@@ -864,7 +866,7 @@ int eb_ctx::setup_persistent() {
     pinfo.inputs_concurrent = inputs_concurrent ? 1 : 0;
     pinfo.inv_dt = 1.0 / dt_s;
     int rc;
-    const size_t bar_words = (size_t)((persist_grid + 15) / 16 + 2) * 32;  // generation, root, one line per group
+    bar_words = (size_t)((persist_grid + 15) / 16 + 2) * 32;  // generation, root, one line per group
     if ((rc = dalloc((void **)&pinfo.bar, bar_words * sizeof(unsigned)))) return rc;
     CK(cudaMemsetAsync(pinfo.bar, 0, bar_words * sizeof(unsigned), stream));
     if ((rc = dalloc((void **)&d_pops, sizeof(PopDev) * (size_t)n_model))) return rc;
@@ -1136,8 +1138,26 @@ int eb_ctx::sync() {
         }
         if (f & FLAG_RECORD_OVERFLOW) { set_error("spike recording buffer full (drain with eb_get_spikes or raise eb_set_record_capacity)"); return EB_ERR_OVERFLOW; }
         if (f & FLAG_SPIKELIST_OVERFLOW) { set_error("internal spike list overflow"); return EB_ERR_OVERFLOW; }
-        if (f & FLAG_BARRIER_TIMEOUT) { set_error("persistent kernel: grid barrier wait timed out"); return EB_ERR_CUDA; }
+        if (f & FLAG_BARRIER_TIMEOUT) {
+            // blocks gave up part-way through a barrier: reset its counters and the
+            // item queues, so the next launch starts from a clean barrier
+            if (pinfo.bar) CK(cudaMemset(pinfo.bar, 0, bar_words * sizeof(unsigned)));
+            if (pinfo.queue) CK(cudaMemset(pinfo.queue, 0, 4 * 16 * sizeof(unsigned long long)));
+            set_error("persistent kernel: grid barrier wait timed out (the run stopped part-way; restore a "
+                      "snapshot before continuing)");
+            return EB_ERR_CUDA;
+        }
+        if (f & FLAG_PERSIST_UNSUPPORTED) { set_error("persistent kernel: integrator outside its compiled class"); return EB_ERR_STATE; }
     }
+    return EB_OK;
+}
+
+int eb_set_barrier_wait(eb_ctx *ctx, uint64_t spin_limit, int withhold_first_block) {
+    if (!ctx || spin_limit == 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    ctx->barrier_spin_limit = spin_limit;
+    ctx->barrier_withhold = withhold_first_block != 0;
+    ctx->pinfo.spin_limit = spin_limit;
+    ctx->pinfo.withhold = withhold_first_block != 0 ? 1 : 0;
     return EB_OK;
 }
 
@@ -1553,6 +1573,23 @@ int eb_set_poisson_rates(eb_ctx *ctx, int64_t first, int64_t n, const float *rat
                           cudaMemcpyHostToDevice));
         }
     }
+    return EB_OK;
+}
+
+int eb_enable_conductances(eb_ctx *ctx, int pop, int mask) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (ctx->finalized) { set_error("eb_enable_conductances after eb_finalize"); return EB_ERR_STATE; }
+    if (pop < 0 || pop >= (int)ctx->pops.size() || mask < 0 || mask > 7) { set_error("bad population or mask"); return EB_ERR_ARG; }
+    ctx->pops[pop].en |= mask;
+    return EB_OK;
+}
+
+int eb_population_state(eb_ctx *ctx, int pop, int var, float **device_ptr) {
+    if (!ctx || !device_ptr) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("eb_population_state before eb_finalize"); return EB_ERR_STATE; }
+    if (pop < 0 || pop >= (int)ctx->pops.size() || var < 0 || var >= kMaxVars) { set_error("bad population or variable"); return EB_ERR_ARG; }
+    const auto &p = ctx->pops[pop];
+    *device_ptr = (p.kind == KIND_INPUT || p.kind == KIND_POISSON || var >= p.dev.nvars) ? nullptr : p.dev.x[var];
     return EB_OK;
 }
 

@@ -53,6 +53,9 @@ struct eb_ctx {
     std::vector<int32_t> stype, rule;
     uint32_t bucket_limit = 8192, input_multiplicity = 2;
     int64_t wide_indegree = 1024;  // block-per-neuron update above this in-degree (0: whenever a bucket holds > 16)
+    unsigned long long barrier_spin_limit = eb::kBarrierSpinLimit;  // persistent kernel: polls per barrier wait
+    bool barrier_withhold = false;  // block 0 withholds its barrier arrivals (failure-path test)
+    size_t bar_words = 0;           // words of pinfo.bar
     uint32_t rng_seed = 1;  // RandomGenerator::srand value (the reference's EDLUTKernel uses 1)
     int64_t rec_cap = 16 << 20;
     // derived

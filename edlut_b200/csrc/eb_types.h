@@ -24,6 +24,7 @@ constexpr uint32_t FLAG_BDF_SINGULAR = 2u;
 constexpr uint32_t FLAG_RECORD_OVERFLOW = 4u;
 constexpr uint32_t FLAG_SPIKELIST_OVERFLOW = 8u;
 constexpr uint32_t FLAG_BARRIER_TIMEOUT = 16u;
+constexpr uint32_t FLAG_PERSIST_UNSUPPORTED = 32u;  // persistent kernel met an integrator outside its class
 
 // One delivery waiting in a target's bucket: the arrival time (double seconds,
 // as the reference computes it) and the synapse, both in source-major order

@@ -131,6 +131,13 @@ int eb_set_graph_steps(eb_ctx *ctx, int graph_steps);
  * which is faster on B200 for the networks measured (a grid barrier over all
  * SMs costs more than the launches it replaces). */
 int eb_set_persistent(eb_ctx *ctx, int on);
+/* The persistent kernel's grid barriers wait at most spin_limit polls (default
+ * 2^24, about a second) before the kernel records a timeout and ends; the run then
+ * returns EB_ERR_CUDA, the barrier counters are reset, and the context stays usable
+ * (restore a snapshot: the run stopped part-way).  withhold_first_block != 0 makes
+ * block 0 skip its barrier arrivals, so every wait runs out: a way to exercise that
+ * failure path without a fault. */
+int eb_set_barrier_wait(eb_ctx *ctx, uint64_t spin_limit, int withhold_first_block);
 /* Timeline of the persistent kernel for the first `steps` steps of each launch:
  * globaltimer (ns) per step, per mark (0 start, 1 phase-A barrier arrival,
  * 2 phase-A barrier exit, 3 phase-B barrier arrival, 4 end of the block's first
@@ -160,6 +167,18 @@ int eb_get_spikes(eb_ctx *ctx, int64_t cap, int64_t *n, int64_t *step, int64_t *
  * append != 0 appends to the file.  Spikes of input neurons, which the caller
  * supplied, are not recorded and not written. */
 int eb_write_spikes(eb_ctx *ctx, const char *path, int append);
+/* Enable conductance types of population `pop` (mask: bit 0 AMPA, 1 GABA, 2 NMDA)
+ * beyond those its synapses enable -- for populations that receive arrivals
+ * folded in from outside (eb_fold_arrivals), such as the neuron-model plugins of a
+ * host engine that delivers spikes itself.  The models integrate and decay the
+ * enabled types only, as the reference CPU models do
+ * (src/neuron_model/LIFTimeDrivenModel.cpp:209-241).  Before eb_finalize. */
+int eb_enable_conductances(eb_ctx *ctx, int pop, int mask);
+/* Device address of state variable `var` (order as eb_get_state) of population
+ * `pop`, or NULL when the variable is not stored; valid until eb_ctx_destroy.  For
+ * device-side ops on the state between runs, e.g. eb_fold_arrivals into the
+ * conductances. */
+int eb_population_state(eb_ctx *ctx, int pop, int var, float **device_ptr);
 /* Output flag of population `pop` (eb_add_population order). */
 int eb_set_output(eb_ctx *ctx, int pop, int on);
 /* Write the weights in network-file order in the reference's weights-file format,

@@ -136,8 +136,9 @@ def ref_available() -> bool:
     return os.path.exists(os.path.join(REF_DIR, "ref_harness"))
 
 
-def run_reference(net, in_times, in_cells, nsteps: int, workdir: str, trace=(0, 0, 0)):
-    """Run the reference EDLUT CPU kernel (oracle/_ref/ref_harness) on the same network.
+def run_reference(net, in_times, in_cells, nsteps: int, workdir: str, trace=(0, 0, 0), exe: str | None = None):
+    """Run the reference EDLUT CPU kernel (oracle/_ref/ref_harness, or the harness
+    binary ``exe`` built against another build of the reference) on the same network.
 
     Returns dict(spike_time, spike_cell, trace[steps, n, nvars], syn (sorted records),
     w_final (original order), counts, of_text / sf_text (bytes of the reference's
@@ -147,7 +148,7 @@ def run_reference(net, in_times, in_cells, nsteps: int, workdir: str, trace=(0, 
     inp = os.path.join(workdir, "inputs.cfg")
     write_input_spikes(inp, in_times, in_cells)
     dt = next(l.dt for l in net.layers if l.model not in ("InputSpikeNeuronModel",))
-    cmd = [os.path.join(REF_DIR, "ref_harness"), os.path.basename(netf), os.path.basename(wf),
+    cmd = [exe or os.path.join(REF_DIR, "ref_harness"), os.path.basename(netf), os.path.basename(wf),
            "inputs.cfg", str(nsteps), repr(float(np.float32(dt))), "out"] + [str(x) for x in trace]
     r = subprocess.run(cmd, cwd=workdir, capture_output=True, text=True)
     if r.returncode != 0:

@@ -180,6 +180,32 @@ def test_bucket_overflow_is_reported_and_context_survives():
     sim.close()
 
 
+def test_persistent_barrier_timeout_is_reported_and_context_recovers():
+    """The persistent kernel's grid-barrier waits are bounded: with block 0 made to
+    withhold its arrivals and a short wait limit, every wait runs out, the run
+    returns an error (no hang, no fault), and after a restore the context runs on
+    to the same result as an undisturbed run."""
+    from edlut_b200._lib import EdlutError
+    net, t, c, nsteps, _ = build_case("cereb_small_rk4")
+    ref, w_ref = run_case("cereb_small_rk4", persistent=True)
+    sim = make_sim(net, persistent=True)
+    sim.inject_spikes(t, c)
+    sim.snapshot(0)
+    L = sim._L
+    assert L.eb_set_barrier_wait(sim._h, 1 << 12, 1) == 0
+    with pytest.raises(EdlutError) as e:
+        sim.run(64)
+    assert e.value.code == -2 and "timed out" in str(e.value)
+    assert L.eb_set_barrier_wait(sim._h, 1 << 24, 0) == 0
+    sim.restore(0)
+    sim.run(nsteps)
+    got = spike_pairs(*sim.spikes())
+    w = sim.weights()
+    sim.close()
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(w, w_ref)
+
+
 def test_bad_calls_return_errors():
     from edlut_b200._lib import EdlutError
     from edlut_b200.simulation import Simulation

@@ -44,7 +44,8 @@ def device_fold(fn, target, stype, weight, time, g0):
     return [x.cpu().numpy() for x in g]
 
 
-@pytest.mark.parametrize("n,m", [(0, 10), (1, 1), (5000, 37), (200000, 3000)])
+# (100000, 1): every arrival on one target, the per-target sort's worst case
+@pytest.mark.parametrize("n,m", [(0, 10), (1, 1), (5000, 37), (200000, 3000), (100000, 1)])
 def test_fold_matches_host_order(n, m):
     from edlut_b200 import _lib
     L = _lib.load()
