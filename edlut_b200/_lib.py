@@ -62,6 +62,9 @@ SIGNATURES = [
     ("eb_get_trace", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
     ("eb_write_spikes", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int]),
     ("eb_set_output", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("eb_set_monitor", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("eb_open_monitor", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int64, ctypes.c_int64]),
+    ("eb_close_monitor", ctypes.c_int, [ctypes.c_void_p]),
     ("eb_save_weights", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p]),
     ("eb_get_weights", ctypes.c_int, [ctypes.c_void_p, c_f32p]),
     ("eb_set_weights", ctypes.c_int, [ctypes.c_void_p, c_f32p]),

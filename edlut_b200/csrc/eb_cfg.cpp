@@ -168,6 +168,7 @@ extern "C" int eb_load_network_files(eb_ctx *ctx, const char *network_file, cons
                 return rc;
         }
         ctx->pops.back().output = outn != 0;
+        ctx->pops.back().monitor = monit != 0 && kind != KIND_INPUT;
     }
     f.skip_comments();
     int nrules = 0;

@@ -156,6 +156,34 @@ __device__ __forceinline__ void apply_pending_post(const PopDev &P, const NetDev
 
 __device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
 
+// State monitor (the reference's -logp): the state after step k and the spike
+// flag of monitored neuron i, at row k % mon_steps.
+__device__ __forceinline__ void monitor_state(const PopDev &P, const NetDev &N, int64_t k, int64_t i, const float *x,
+                                              int nv, bool sp) {
+    const int64_t o = (k % N.mon_steps) * N.mon_n + P.mon_base + i;
+    float *d = N.mon_x + o * kMaxVars;
+    for (int v = 0; v < nv; ++v) d[v] = x[v];
+    N.mon_spk[o] = sp ? 1 : 0;
+}
+
+// A delivery of weight w (type ty) into monitored neuron i, folded by step k.
+__device__ __forceinline__ void monitor_delivery(const PopDev &P, const NetDev &N, int64_t k, int64_t i,
+                                                 const Arrival &v, int ty, float w) {
+    const unsigned long long o = atomicAdd(N.mon_count, 1ull);
+    if (o < (unsigned long long)N.mon_cap) {
+        MonDelivery d;
+        d.a = v.a;
+        d.spos = v.spos;
+        d.cell = (uint32_t)(P.mon_base + i);
+        d.w = w;
+        d.ty = ty;
+        d.k = k;
+        N.mon_del[o] = d;
+    } else {
+        atomicOr(N.flags, FLAG_MONITOR_OVERFLOW);
+    }
+}
+
 template <int ND>
 __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
     if (ty == 0) x[ND] += w;
@@ -166,11 +194,13 @@ __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
 // Apply one arrival at neuron i: g[type] += w (weight before plasticity), then
 // STDP pre (after the target's deferred post updates, when it keeps a ring).
 template <int ND>
-__device__ __forceinline__ void apply_arrival(const PopDev &P, const NetDev &N, int64_t i, const Arrival &r, float *x) {
+__device__ __forceinline__ void apply_arrival(const PopDev &P, const NetDev &N, int64_t k, int64_t i, const Arrival &r,
+                                              float *x) {
     const uint32_t tp = r.tpos;
     SynRec s = N.syn[tp];
     if (s.rule >= 0 && P.post_t) apply_pending_post(P, N, i, s);
     add_conductance<ND>(x, s.stype, s.w);
+    if (P.mon) monitor_delivery(P, N, k, i, r, s.stype, s.w);
     if (s.rule >= 0) stdp_pre(N, tp, s, r.a);
 }
 
@@ -390,7 +420,7 @@ __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, in
             if (c > capg) { atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
             Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
             if (c == 1) {
-                apply_arrival<ND>(P, N, i, r[0], x);
+                apply_arrival<ND>(P, N, k, i, r[0], x);
             } else if (c <= kLocalSort) {
                 Arrival loc[kLocalSort];
                 for (uint32_t a = 0; a < c; ++a) {
@@ -399,7 +429,7 @@ __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, in
                     while (b >= 0 && arr_less(v, loc[b])) { loc[b + 1] = loc[b]; --b; }
                     loc[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, loc[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, loc[a], x);
             } else {
                 for (uint32_t a = 1; a < c; ++a) {  // in-place insertion sort (rare path)
                     Arrival v = r[a];
@@ -407,11 +437,12 @@ __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, in
                     while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
                     r[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, r[a], x);
             }
         }
         sp = advance_neuron<KIND, INTEG, EN>(P, N, i, x, ax);
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
+        if (P.mon) monitor_state(P, N, k, i, x, Model<KIND>::NV, sp);
         if (sp && P.post_t) note_post_spike(P, N, i, k);
     }
     // delivered-event counter: one atomic per warp
@@ -679,7 +710,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                 if (own) S.sbuf[S.rank[tid]] = v;
                 __syncthreads();
                 if (tid == 0)
-                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, S.sbuf[a], x);
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, S.sbuf[a], x);
             } else {
                 if (own) {
                     if (rec.rule >= 0) {
@@ -690,6 +721,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                         S.sw[S.rank[tid]] = rec.w;
                     }
                     S.sty[S.rank[tid]] = rec.stype;
+                    if (P.mon) monitor_delivery(P, N, k, i, v, rec.stype, S.sw[S.rank[tid]]);
                 }
                 wide_fold<ND>(S, x, c);
             }
@@ -717,7 +749,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                 }
             if (P.may_repeat) {
                 if (tid == 0)
-                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, S.sbuf[a], x);
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, S.sbuf[a], x);
             } else {
                 for (int a = tid; a < (int)c; a += nt) {
                     const Arrival v = S.sbuf[a];
@@ -726,6 +758,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                     stdp_pre_gather(P, N, i, v.tpos, v.a, w_old, ty);
                     S.sw[a] = w_old;
                     S.sty[a] = (uint8_t)ty;
+                    if (P.mon) monitor_delivery(P, N, k, i, v, ty, w_old);
                 }
                 __syncthreads();
                 wide_fold<ND>(S, x, c);
@@ -741,7 +774,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                     while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
                     r[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, i, r[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, r[a], x);
             }
         }
         if (tid == 0) atomicAdd(P.events, (unsigned long long)c);
@@ -762,6 +795,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
             }
         }
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
+        if (P.mon) monitor_state(P, N, k, i, x, Model<KIND>::NV, sp);
         if (sp) {
             if (list) {
                 const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
@@ -905,6 +939,7 @@ __device__ __forceinline__ int wide_advance(const PopDev &P, const NetDev &N, in
         if (P.post_f) S.ring_f[q] = P.post_f[i * kPostRing + q];
     }
     record_trace(P, N, ks, gi, x, Model<KIND>::NV);
+    if (P.mon) monitor_state(P, N, ks, i, x, Model<KIND>::NV, sp != 0);
     if (sp) {
         if (list) {
             const uint32_t o = atomicAdd(&P.spk_count[ks & 1], 1u);
@@ -1022,6 +1057,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                     const uint32_t pos = S.woff[stage_step_of(S, s0, a0 + a)] - a0 + G.rank[a];
                     S.sw[pos] = r.w;
                     S.sty[pos] = r.stype;
+                    if (P.mon) monitor_delivery(P, N, k + stage_step_of(S, s0, a0 + a), i, G.arr[a], r.stype, r.w);
                     if (r.rule >= 0) stdp_pre_rec(N, r, G.arr[a].a);
                     G.rec[a] = r;
                 }
@@ -1053,6 +1089,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                     if (r.rule >= 0 && ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, prule, r);
                     S.sw[o0 + G.rank[a]] = r.w;
                     S.sty[o0 + G.rank[a]] = r.stype;
+                    if (P.mon) monitor_delivery(P, N, ks, i, G.arr[a], r.stype, r.w);
                     if (r.rule >= 0) {
                         stdp_pre_rec(N, r, G.arr[a].a);
                         sr = r;

@@ -1148,6 +1148,11 @@ int eb_ctx::sync() {
             return EB_ERR_CUDA;
         }
         if (f & FLAG_PERSIST_UNSUPPORTED) { set_error("persistent kernel: integrator outside its compiled class"); return EB_ERR_STATE; }
+        if (f & FLAG_MONITOR_OVERFLOW) {
+            set_error("state monitor: more deliveries into monitored neurons in one chunk than its log holds "
+                      "(raise the delivery capacity of eb_open_monitor)");
+            return EB_ERR_OVERFLOW;
+        }
     }
     return EB_OK;
 }
@@ -1218,6 +1223,7 @@ eb_ctx::~eb_ctx() {
     for (auto e : join_ev) cudaEventDestroy(e);
     for (auto &r : prof_pending) { ev_pool.push_back(r.a); ev_pool.push_back(r.b); }
     for (auto e : ev_pool) cudaEventDestroy(e);
+    if (mon_file) std::fclose(mon_file);
     dfree_all();
     if (rec_host) cudaFreeHost(rec_host);
     if (own_stream && stream) cudaStreamDestroy(stream);
@@ -1375,6 +1381,7 @@ int eb_set_graph_steps(eb_ctx *ctx, int graph_steps) {
 
 int eb_run_async(eb_ctx *ctx, int64_t n_steps) {
     if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (ctx->mon_file) { set_error("eb_run_async while the state monitor is open (eb_run writes it)"); return EB_ERR_STATE; }
     CK(cudaSetDevice(ctx->device));
     return ctx->run_async(n_steps);
 }
@@ -1385,6 +1392,10 @@ int eb_sync(eb_ctx *ctx) {
 }
 
 int eb_run(eb_ctx *ctx, int64_t n_steps) {
+    if (ctx && ctx->mon_file) {
+        CK(cudaSetDevice(ctx->device));
+        return ctx->run_monitored(n_steps);
+    }
     int rc = eb_run_async(ctx, n_steps);
     if (rc) return rc;
     return ctx->sync();
@@ -1597,6 +1608,204 @@ int eb_set_output(eb_ctx *ctx, int pop, int on) {
     if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
     if (pop < 0 || pop >= (int)ctx->pops.size()) { set_error("population %d out of range", pop); return EB_ERR_ARG; }
     ctx->pops[pop].output = on != 0;
+    return EB_OK;
+}
+
+int eb_set_monitor(eb_ctx *ctx, int pop, int on) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    if (pop < 0 || pop >= (int)ctx->pops.size()) { set_error("population %d out of range", pop); return EB_ERR_ARG; }
+    ctx->pops[pop].monitor = on != 0;
+    return EB_OK;
+}
+
+// The state monitor of the reference's -logp option: Simulation::WriteState
+// (src/simulation/Simulation.cpp:397-405) into FileOutputSpikeDriver::WriteState
+// (src/communication/FileOutputSpikeDriver.cpp:48-62) for the neurons of layers
+// with the log column set (src/spike/Network.cpp:1102-1108).  The kernels keep
+// each step's state of the monitored neurons and a log of the deliveries into
+// them (weight and conductance type, in fold order); the host writes the lines
+// after each chunk of steps.
+int eb_open_monitor(eb_ctx *ctx, const char *path, int64_t chunk_steps, int64_t delivery_capacity) {
+    if (!ctx || !path || chunk_steps < 0 || delivery_capacity < 0) { set_error("bad argument"); return EB_ERR_ARG; }
+    if (!ctx->finalized) { set_error("eb_open_monitor before eb_finalize"); return EB_ERR_STATE; }
+    int rc;
+    if ((rc = ctx->close_monitor())) return rc;
+    CK(cudaSetDevice(ctx->device));
+    ctx->mon_cell.clear();
+    ctx->mon_pop.clear();
+    for (int q = 0; q < (int)ctx->pops.size(); ++q) {
+        HostPop &p = ctx->pops[q];
+        const bool on = p.monitor && (p.kind == KIND_LIF || p.kind == KIND_ADEX || p.kind == KIND_HH);
+        p.dev.mon = on ? 1 : 0;
+        p.dev.mon_base = on ? (int64_t)ctx->mon_cell.size() : 0;
+        if (on)
+            for (int64_t i = 0; i < p.n; ++i) {
+                ctx->mon_cell.push_back(p.first + i);
+                ctx->mon_pop.push_back(q);
+            }
+    }
+    const int64_t n = (int64_t)ctx->mon_cell.size();
+    const int64_t row = (int64_t)(sizeof(float) * kMaxVars + 1);
+    const int64_t steps = chunk_steps ? chunk_steps
+                                      : std::max<int64_t>(8, std::min<int64_t>(4096, (int64_t(64) << 20) / (row * std::max<int64_t>(n, 1))));
+    const int64_t cap = delivery_capacity ? delivery_capacity : (int64_t(1) << 20);
+    NetDev &N = ctx->net;
+    if (n) {
+        if ((rc = ctx->dalloc((void **)&N.mon_x, sizeof(float) * kMaxVars * (size_t)(steps * n))) ||
+            (rc = ctx->dalloc((void **)&N.mon_spk, (size_t)(steps * n))) ||
+            (rc = ctx->dalloc((void **)&N.mon_del, sizeof(MonDelivery) * (size_t)cap)) ||
+            (rc = ctx->dalloc((void **)&N.mon_count, sizeof(unsigned long long)))) {
+            ctx->close_monitor();
+            return rc;
+        }
+        N.mon_n = n;
+        N.mon_steps = steps;
+        N.mon_cap = cap;
+    }
+    ctx->mon_file = std::fopen(path, "w");
+    if (!ctx->mon_file) {
+        ctx->close_monitor();
+        set_error("cannot open %s for writing", path);
+        return EB_ERR_ARG;
+    }
+    ctx->mon_steps = steps;
+    ctx->mon_cap = cap;
+    ctx->mon_cur.assign((size_t)n * kMaxVars, 0.0f);
+    ctx->graphs_valid = false;
+    ctx->pops_dirty = true;
+    return EB_OK;
+}
+
+int eb_close_monitor(eb_ctx *ctx) {
+    if (!ctx) { set_error("null context"); return EB_ERR_ARG; }
+    return ctx->close_monitor();
+}
+
+int eb_ctx::close_monitor() {
+    bool bad = false;
+    if (mon_file) {
+        bad = std::fclose(mon_file) != 0;
+        mon_file = nullptr;
+    }
+    if (net.mon_x || net.mon_del) {
+        CK(cudaStreamSynchronize(stream));
+        dfree(net.mon_x);
+        dfree(net.mon_spk);
+        dfree(net.mon_del);
+        dfree(net.mon_count);
+    }
+    net.mon_x = nullptr;
+    net.mon_spk = nullptr;
+    net.mon_del = nullptr;
+    net.mon_count = nullptr;
+    net.mon_n = net.mon_steps = net.mon_cap = 0;
+    bool was_on = false;
+    for (auto &p : pops) {
+        was_on |= p.dev.mon != 0;
+        p.dev.mon = 0;
+        p.dev.mon_base = 0;
+    }
+    if (was_on) {
+        graphs_valid = false;
+        pops_dirty = true;
+    }
+    mon_cell.clear();
+    mon_pop.clear();
+    mon_cur.clear();
+    if (bad) { set_error("write to the state monitor file failed"); return EB_ERR_ARG; }
+    return EB_OK;
+}
+
+// eb_run with the monitor open: chunks of at most mon_steps steps, each followed
+// by its lines.  The host copy of the monitored states starts every chunk from
+// the device state, so states set between runs show up.
+int eb_ctx::run_monitored(int64_t n) {
+    const int64_t nm = (int64_t)mon_cell.size();
+    std::vector<float> col;
+    while (n > 0) {
+        const int64_t c = std::min(n, mon_steps), k0 = steps_done;
+        int rc;
+        if (nm) {
+            CK(cudaStreamSynchronize(stream));
+            for (int64_t j = 0; j < nm;) {
+                const HostPop &p = pops[mon_pop[j]];
+                col.resize((size_t)p.n);
+                for (int v = 0; v < kMaxVars; ++v) {
+                    if (v < p.dev.nvars && p.dev.x[v])
+                        CK(cudaMemcpy(col.data(), p.dev.x[v], sizeof(float) * (size_t)p.n, cudaMemcpyDeviceToHost));
+                    else
+                        std::fill(col.begin(), col.end(), 0.0f);
+                    for (int64_t i = 0; i < p.n; ++i) mon_cur[(size_t)(j + i) * kMaxVars + v] = col[(size_t)i];
+                }
+                j += p.n;
+            }
+            CK(cudaMemsetAsync(net.mon_count, 0, sizeof(unsigned long long), stream));
+        }
+        if ((rc = run_async(c))) return rc;
+        if ((rc = sync())) return rc;
+        if (nm && (rc = write_monitor(k0, c))) return rc;
+        n -= c;
+    }
+    return EB_OK;
+}
+
+// Lines of steps k0+1 .. k0+n: before each step's lines, the deliveries it folded
+// in (time, synapse order), each after its weight is added to the host copy in
+// that order (the device's float additions); then per monitored population the
+// neurons that spiked and all its neurons, after the step.
+int eb_ctx::write_monitor(int64_t k0, int64_t n) {
+    const int64_t nm = (int64_t)mon_cell.size();
+    unsigned long long cnt = 0;
+    CK(cudaMemcpy(&cnt, net.mon_count, sizeof(cnt), cudaMemcpyDeviceToHost));
+    if (cnt > (unsigned long long)mon_cap) { set_error("state monitor delivery log overflow"); return EB_ERR_OVERFLOW; }
+    std::vector<MonDelivery> del((size_t)cnt);
+    if (cnt) CK(cudaMemcpy(del.data(), net.mon_del, sizeof(MonDelivery) * (size_t)cnt, cudaMemcpyDeviceToHost));
+    std::sort(del.begin(), del.end(), [](const MonDelivery &x, const MonDelivery &y) {
+        if (x.k != y.k) return x.k < y.k;
+        if (x.a != y.a) return x.a < y.a;
+        if (x.spos != y.spos) return x.spos < y.spos;
+        return x.cell < y.cell;
+    });
+    std::vector<float> xs((size_t)(mon_steps * nm) * kMaxVars);
+    std::vector<uint8_t> sp((size_t)(mon_steps * nm));
+    CK(cudaMemcpy(xs.data(), net.mon_x, sizeof(float) * xs.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sp.data(), net.mon_spk, sp.size(), cudaMemcpyDeviceToHost));
+    std::FILE *f = mon_file;
+    bool ok = true;
+    auto line = [&](float t, int64_t j) {
+        const HostPop &p = pops[mon_pop[j]];
+        const float *x = &mon_cur[(size_t)j * kMaxVars];
+        ok &= std::fprintf(f, "%f\t%li", (double)t, (long)mon_cell[j]) > 0;
+        for (int v = 0; v < p.dev.nvars; ++v) ok &= std::fprintf(f, "\t%1.12f", (double)x[v]) > 0;
+        // the reference's external-current variable (no current synapses on this
+        // path), the last-update time a time-driven model never sets, and the two
+        // event-driven fields a time-driven model prints as -1
+        // (src/neuron_model/VectorNeuronState.cpp:193-209)
+        ok &= std::fprintf(f, "\t%1.12f\t%1.12f\t%1.12f\t%1.12f\n", 0.0, 0.0, -1.0, -1.0) > 0;
+    };
+    size_t d = 0;
+    while (d < del.size() && del[d].k <= k0) ++d;  // none expected
+    for (int64_t k = k0 + 1; k <= k0 + n && ok; ++k) {
+        for (; d < del.size() && del[d].k == k; ++d) {
+            const MonDelivery &e = del[d];
+            const int nd = pops[mon_pop[e.cell]].dev.ndiff;
+            mon_cur[(size_t)e.cell * kMaxVars + nd + e.ty] += e.w;
+            line((float)e.a, (int64_t)e.cell);
+        }
+        const int64_t row = k % mon_steps;
+        std::copy(xs.begin() + (size_t)(row * nm) * kMaxVars, xs.begin() + (size_t)((row + 1) * nm) * kMaxVars,
+                  mon_cur.begin());
+        double t = 0.0;
+        eb_step_time(this, k, &t);
+        for (int64_t j = 0; j < nm;) {
+            const int64_t e = j + pops[mon_pop[j]].n;
+            for (int64_t i = j; i < e; ++i)
+                if (sp[(size_t)(row * nm + i)]) line((float)t, i);
+            for (int64_t i = j; i < e; ++i) line((float)t, i);
+            j = e;
+        }
+    }
+    if (!ok) { set_error("write to the state monitor file failed"); return EB_ERR_ARG; }
     return EB_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <array>
 #include <functional>
 #include <cstdint>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,7 @@ struct HostPop {
     int en = 0;                 // enabled conductance types (from the synapse types targeting it)
     bool has_out = false, has_plastic_in = false;
     bool output = true;         // spikes go to eb_write_spikes (the layer line's output column)
+    bool monitor = false;       // states go to the state monitor file (the layer line's log column)
     int post_chunks = 1;
     int push_threads = 32;
     std::vector<float> rates;   // Poisson generators: per-neuron frequency (Hz)
@@ -138,6 +140,13 @@ struct eb_ctx {
     // dynamic device state (what a snapshot copies): (pointer, bytes)
     std::vector<std::pair<void *, size_t>> dyn;
     std::vector<std::pair<int, std::vector<void *>>> snapshots;
+    // state monitor file (the reference's -logp): the file, the global neuron and
+    // population of each monitored index, and the host copy of their states
+    std::FILE *mon_file = nullptr;
+    std::vector<int64_t> mon_cell;
+    std::vector<int> mon_pop;
+    std::vector<float> mon_cur;           // [mon_n][kMaxVars]
+    int64_t mon_steps = 0, mon_cap = 0;
     struct HostSnap { int slot; int64_t steps_done, spikes_drained; int steps_since_flush; };
     std::vector<HostSnap> snap_host;
 
@@ -167,6 +176,9 @@ struct eb_ctx {
     bool lazy_post = false;       // some population defers post-synaptic STDP
     int steps_since_flush = 0;
     int run_async(int64_t n);
+    int run_monitored(int64_t n);
+    int write_monitor(int64_t k0, int64_t n);
+    int close_monitor();
     int sync();
     int snapshot(int slot);
     int restore(int slot);

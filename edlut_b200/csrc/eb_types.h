@@ -25,6 +25,7 @@ constexpr uint32_t FLAG_RECORD_OVERFLOW = 4u;
 constexpr uint32_t FLAG_SPIKELIST_OVERFLOW = 8u;
 constexpr uint32_t FLAG_BARRIER_TIMEOUT = 16u;
 constexpr uint32_t FLAG_PERSIST_UNSUPPORTED = 32u;  // persistent kernel met an integrator outside its class
+constexpr uint32_t FLAG_MONITOR_OVERFLOW = 64u;     // more deliveries into monitored neurons than the log holds
 
 // One delivery waiting in a target's bucket: the arrival time (double seconds,
 // as the reference computes it) and the synapse, both in source-major order
@@ -55,6 +56,19 @@ struct alignas(32) SynRec {
     uint8_t pad[6];
 };
 static_assert(sizeof(SynRec) == 32, "SynRec is one sector");
+
+// One delivery into a monitored neuron: its time and synapse (the fold order
+// within a step is (a, spos)), the neuron's index in the monitored list, the
+// conductance type and the weight it added, and the step that folded it.
+struct alignas(32) MonDelivery {
+    double a;
+    uint32_t spos;
+    uint32_t cell;
+    float w;
+    int32_t ty;
+    int64_t k;
+};
+static_assert(sizeof(MonDelivery) == 32, "MonDelivery is one sector");
 
 // Per-population parameters, passed by value to the kernels.
 struct PopDev {
@@ -100,6 +114,10 @@ struct PopDev {
     DecayPair *post_f;
     int post_rule;
     uint32_t *flush_list;  // [n + 1]: neurons a flush takes, their count last (zero between flushes)
+    // state monitor: nonzero when the population's neurons are monitored; their
+    // first index in the monitored list
+    int mon;
+    int64_t mon_base;
 };
 
 // Network-wide device pointers, passed by value to the kernels.
@@ -141,6 +159,14 @@ struct NetDev {
     int64_t trace_first, trace_n, trace_k0, trace_steps;
     unsigned long long *events;  // delivered synaptic events, one counter per population
     uint32_t *flags;
+    // state monitor: each step's state and spike flag of the monitored neurons at
+    // row k % mon_steps, and the log of deliveries into them
+    float *mon_x;                // [mon_steps][mon_n][kMaxVars]
+    uint8_t *mon_spk;            // [mon_steps][mon_n]
+    int64_t mon_n, mon_steps;
+    MonDelivery *mon_del;
+    unsigned long long *mon_count;
+    int64_t mon_cap;
 };
 
 }  // namespace eb

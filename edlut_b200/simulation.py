@@ -60,9 +60,11 @@ class Simulation:
     @classmethod
     def from_description(cls, net: NetworkDescription, device: int = 0, **kw) -> "Simulation":
         sim = cls(device=device, **kw)
-        for layer in net.layers:
+        for q, layer in enumerate(net.layers):
             sim.add_population(layer.model, layer.n, layer.integrator, layer.bdf_order, layer.dt,
                                layer.full_params() if layer.model in MODEL_PARAM_ORDER else None)
+            if layer.log:
+                sim.set_monitor(q, True)
         for name, params in net.rules:
             if name != "STDP":
                 raise NotImplementedError("learning rule %s is outside this path (only STDP)" % name)
@@ -193,6 +195,18 @@ class Simulation:
 
     def set_output(self, pop: int, on: bool = True) -> None:
         check(self._L.eb_set_output(self._h, int(pop), int(bool(on))))
+
+    def set_monitor(self, pop: int, on: bool = True) -> None:
+        """Monitor the states of population `pop` (the layer line's log column)."""
+        check(self._L.eb_set_monitor(self._h, int(pop), int(bool(on))))
+
+    def open_monitor(self, path: str, chunk_steps: int = 0, delivery_capacity: int = 0) -> None:
+        """Write the monitored populations' states to `path` in the reference's -logp
+        format as the following runs advance (``run`` only, not ``run_async``)."""
+        check(self._L.eb_open_monitor(self._h, os.fsencode(path), int(chunk_steps), int(delivery_capacity)))
+
+    def close_monitor(self) -> None:
+        check(self._L.eb_close_monitor(self._h))
 
     def save_weights(self, path: str) -> None:
         """Write the weights in the reference's weights-file format (-sf)."""

@@ -181,6 +181,27 @@ int eb_enable_conductances(eb_ctx *ctx, int pop, int mask);
 int eb_population_state(eb_ctx *ctx, int pop, int var, float **device_ptr);
 /* Output flag of population `pop` (eb_add_population order). */
 int eb_set_output(eb_ctx *ctx, int pop, int on);
+/* State-monitor flag of population `pop` (the log column of the network file's
+ * layer line; eb_add_population: clear).  Takes effect at the next
+ * eb_open_monitor; input populations are never monitored, as in the reference
+ * (src/spike/Network.cpp:1102-1108). */
+int eb_set_monitor(eb_ctx *ctx, int pop, int on);
+/* Write the states of the monitored neurons to a text file in the reference's
+ * state-monitor format, FileOutputSpikeDriver::WriteState
+ * (src/communication/FileOutputSpikeDriver.cpp:48-62, the -logp option), as every
+ * following eb_run advances: one "%f\t%li" + "\t%1.12f" x (variables + 3) line
+ * (time, neuron, the model's state variables, last-update time 0 and -1 -1 for a
+ * time-driven model) at each delivery into a monitored neuron, after the weight
+ * is added (src/spike/PropagatedSpikeGroup.cpp:73-85, PropagatedSpike.cpp:74-84),
+ * and after each step a line per monitored neuron that spiked, then one per
+ * monitored neuron (src/spike/TimeDrivenInternalSpike.cpp:66-72,113-131).  Runs
+ * advance in chunks of `chunk_steps` steps (0: sized from the monitored
+ * neurons); `delivery_capacity` bounds the deliveries into monitored neurons per
+ * chunk (0: 1M; more returns EB_ERR_OVERFLOW).  After eb_finalize; eb_run_async
+ * is refused while the file is open. */
+int eb_open_monitor(eb_ctx *ctx, const char *path, int64_t chunk_steps, int64_t delivery_capacity);
+/* Flush and close the state-monitor file (also done by eb_ctx_destroy). */
+int eb_close_monitor(eb_ctx *ctx);
 /* Write the weights in network-file order in the reference's weights-file format,
  * Network::SaveWeights (src/spike/Network.cpp:1165-1202, the -sf option): runs of
  * equal weights as "%i %g" lines.  The file loads back with eb_load_network_files. */

@@ -141,8 +141,8 @@ def run_reference(net, in_times, in_cells, nsteps: int, workdir: str, trace=(0, 
     binary ``exe`` built against another build of the reference) on the same network.
 
     Returns dict(spike_time, spike_cell, trace[steps, n, nvars], syn (sorted records),
-    w_final (original order), counts, of_text / sf_text (bytes of the reference's
-    output-spike and saved-weights files))."""
+    w_final (original order), counts, of_text / sf_text / logp_text (bytes of the
+    reference's output-spike, saved-weights and state-monitor files))."""
     from edlut_b200.network import write_input_spikes
     netf, wf = net.write_files(workdir)
     inp = os.path.join(workdir, "inputs.cfg")
@@ -168,7 +168,7 @@ def run_reference(net, in_times, in_cells, nsteps: int, workdir: str, trace=(0, 
     with open(os.path.join(workdir, "out.counts")) as f:
         out["counts"] = [int(x) for x in f.read().split()]
     # the reference's own output files: spikes (-of) and weights (-sf)
-    for key, ext in (("of_text", ".of"), ("sf_text", ".sf")):
+    for key, ext in (("of_text", ".of"), ("sf_text", ".sf"), ("logp_text", ".logp")):
         path = os.path.join(workdir, "out" + ext)
         if os.path.exists(path):
             with open(path, "rb") as f:

@@ -12,6 +12,8 @@
 //   <out>.wfinal   int64 m, then m float32 final weights in network-file order
 //   <out>.counts   text: spikes propagated_events
 //   <out>.of       text: the reference's own FileOutputSpikeDriver file (-of)
+//   <out>.logp     text: the reference's own state monitor file (-logp), the states
+//                  of the neurons of layers whose log column is set, every step
 //   <out>.sf       text: the reference's own Network::SaveWeights file (-sf)
 //
 // Usage: ref_harness net.cfg weights.cfg inputs.cfg|- nsteps dt_s out_prefix
@@ -70,6 +72,8 @@ int main(int argc, char **argv) {
         sim.AddOutputSpikeDriver(outdrv);
         FileOutputSpikeDriver *filedrv = new FileOutputSpikeDriver((out + ".of").c_str(), false);
         sim.AddOutputSpikeDriver(filedrv);
+        FileOutputSpikeDriver *logdrv = new FileOutputSpikeDriver((out + ".logp").c_str(), true);
+        sim.AddMonitorActivityDriver(logdrv);
         sim.InitSimulation();
 
         Network *nw = sim.GetNetwork();
@@ -133,6 +137,7 @@ int main(int argc, char **argv) {
 
         nw->SaveWeights((out + ".sf").c_str());
         std::fflush(filedrv->Handler);
+        std::fflush(logdrv->Handler);
 
         std::ofstream fc(out + ".counts");
         fc << sim.GetTotalSpikeCounter() << " " << sim.GetTotalPropagateCounter() << "\n";

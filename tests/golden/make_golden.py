@@ -94,10 +94,23 @@ BIG_CASES = {
 # step's spikes in neuron order
 FILE_CASES = ("adex_rk4_stdp",)
 
+# cases whose model layer has its log column set; the reference's -logp state
+# monitor file (every state variable of every neuron of the layer, each step) is
+# kept as <case>.logp.gz.  Small networks: the file grows with neurons x steps.
+for _m, _i in (("LIFTimeDrivenModel", "RK2"), ("AdExTimeDrivenModel", "RK4"), ("HHTimeDrivenModel", "BDF")):
+    CASES["%s_logp" % _m[:-15].lower()] = (
+        "parity_network", dict(model=_m, integrator=_i, bdf_order=2, n=24, n_inputs=12, stdp=True, seed=8, rate_hz=300.0,
+                               delays=(1e-3, 2e-3), dt=5e-5 if _m.startswith("HH") else 1e-4), 200, (200, 12, 6))
+LOG_CASES = ("lif_logp", "adex_logp", "hh_logp")
+
 
 def build_case(name: str):
     builder, kw, nsteps, trace = CASES[name] if name in CASES else BIG_CASES[name]
     net, t, c = getattr(C, builder)(**kw)
+    if name in LOG_CASES:
+        for layer in net.layers:
+            if layer.model != "InputSpikeNeuronModel":
+                layer.log = 1
     return net, t, c, nsteps, trace
 
 
@@ -150,11 +163,12 @@ def make(name: str) -> dict:
         out["w_final"] = R["w_final"].astype(np.float32)
     out["perm_sha256"] = np.array(perm_digest(R["syn"]["orig"]))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
-    if name in FILE_CASES:
-        import gzip
-        for key, ext in (("of_text", ".of.gz"), ("sf_text", ".sf.gz")):
-            with gzip.GzipFile(os.path.join(HERE, name + ext), "wb", mtime=0) as f:
-                f.write(R[key])
+    import gzip
+    keep = ((("of_text", ".of.gz"), ("sf_text", ".sf.gz")) if name in FILE_CASES else ()) + \
+        ((("logp_text", ".logp.gz"),) if name in LOG_CASES else ())
+    for key, ext in keep:
+        with gzip.GzipFile(os.path.join(HERE, name + ext), "wb", mtime=0) as f:
+            f.write(R[key])
     return dict(spikes=int(len(steps)), counts=[int(x) for x in R["counts"]])
 
 

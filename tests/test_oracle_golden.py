@@ -72,3 +72,45 @@ def test_fixture_dynamics_are_finite():
             assert not np.isfinite(tr).all(), name
         else:
             assert np.isfinite(tr).all(), name
+
+
+def test_reference_monitor_files_agree_with_fixture():
+    """The reference's own -logp state-monitor file kept for a case agrees with its
+    binary fixture: after each step, a line per neuron that spiked then a line per
+    monitored neuron, at the step's update time, whose membrane potentials are the
+    fixture's trace; between the steps one line per delivered synaptic event."""
+    from oracle.oracle import step_times
+    from tests._cases import load_golden_text
+    from tests.golden.make_golden import LOG_CASES
+    for name in LOG_CASES:
+        g = load_golden(name)
+        net, t, c, nsteps, (tsteps, tfirst, tn) = build_case(name)
+        dt = next(l.dt for l in net.layers if l.model != "InputSpikeNeuronModel")
+        ts = step_times(dt, nsteps)
+        mon, first = [], 0
+        for l in net.layers:
+            if l.model != "InputSpikeNeuronModel":
+                mon.extend(range(first, first + l.n))
+            first += l.n
+        rows = [ln.split("\t") for ln in load_golden_text(name, ".logp").decode().splitlines()]
+        spikes = {}
+        for s, cell in spike_pairs(g["spike_step"], g["spike_cell"]).tolist():
+            spikes.setdefault(s, []).append(cell)
+        i, deliveries = 0, 0
+        for k in range(1, nsteps + 1):
+            tk = "%f" % float(np.float32(ts[k]))
+            want = spikes.get(k, []) + mon
+            while [int(r[1]) for r in rows[i:i + len(want)]] != want or any(r[0] != tk for r in rows[i:i + len(want)]):
+                assert int(rows[i][1]) in mon
+                assert float(ts[k - 1]) - 1e-6 <= float(rows[i][0]) <= float(ts[k]) + 1e-6
+                deliveries += 1
+                i += 1
+            block = {int(r[1]): r for r in rows[i + len(want) - len(mon):i + len(want)]}
+            for r in rows[i:i + len(want) - len(mon)]:
+                assert r == block[int(r[1])]
+            if k <= tsteps:
+                v = ["%1.12f" % float(x) for x in g["trace"][k - 1, :, 0]]
+                assert [block[cell][2] for cell in range(tfirst, tfirst + tn)] == v
+            i += len(want)
+        deliveries += len(rows) - i
+        assert deliveries == int(g["counts"][1])
