@@ -8,8 +8,8 @@ spike neurons, device Poisson generators and STDP runs unchanged after
 dictionary keys ('int_meth', 'weight', 'max_weight', 'type', 'delay', 'wchange',
 'trigger_wchange'), returned index lists and spike-activity tuples.  What the
 path does not cover (other neuron models, current inputs, trigger learning rules,
-monitor and weight-file drivers) raises ``NotImplementedError`` naming the call,
-where the reference would run it on the CPU.
+weight-file drivers) raises ``NotImplementedError`` naming the call, where the
+reference would run it on the CPU.
 
 As in the reference, layers, learning rules and synaptic layers are only
 registered until ``Initialize``; spikes injected before ``Initialize`` are kept
@@ -62,6 +62,9 @@ class PySimulation_API:
         self._spikes_c: List[int] = []
         self._out_files: List[str] = []
         self._output_pop: List[bool] = []
+        self._log_pop: List[bool] = []
+        self._mon_spike_files: List[str] = []
+        self._mon_state_file = None
 
     # ------------------------------------------------------------ catalogue --
     def GetAvailableNeuronModels(self) -> List[str]:
@@ -127,6 +130,7 @@ class PySimulation_API:
         r = self._net.add_layer(Layer(int(num_neurons), model_name, params, output=int(bool(output_activity)),
                                       log=int(bool(log_activity)), **kw))
         self._output_pop.append(bool(output_activity))
+        self._log_pop.append(bool(log_activity) and model_name not in INPUT_MODELS)
         return list(r)
 
     def AddLearningRule(self, model_name: str, param_dict: Dict[str, float]) -> int:
@@ -172,12 +176,31 @@ class PySimulation_API:
         with open(file_name, "w"):
             pass
 
+    def AddFileOutputMonitorDriver(self, file_name: str, monitor_state: bool) -> None:
+        """A monitor file for the layers added with log_activity
+        (Simulation_API::AddFileOutputMonitorDriver, src/simulation/Simulation_API.cpp:263):
+        monitor_state true writes their states in the -logp format (a line at each
+        delivery into a monitored neuron and after each step, see
+        ``Simulation.open_monitor``); false writes their spikes in the -of format.
+        One state file per simulation."""
+        self._check_open("AddFileOutputMonitorDriver")
+        if monitor_state:
+            if self._mon_state_file is not None:
+                raise NotImplementedError("AddFileOutputMonitorDriver: one state monitor file per simulation")
+            self._mon_state_file = str(file_name)
+        else:
+            self._mon_spike_files.append(str(file_name))
+        with open(file_name, "w"):
+            pass
+
     def Initialize(self) -> None:
         self._check_open("Initialize")
         from .simulation import Simulation
         self._sim = Simulation.from_description(self._net, random_seed=self._seed)
         for q, on in enumerate(self._output_pop):
             self._sim.set_output(q, on)
+        if self._mon_state_file is not None:
+            self._sim.open_monitor(self._mon_state_file)
         for t, c in self._pending_in:
             self._sim.inject_spikes(t, c)
         self._pending_in.clear()
@@ -201,7 +224,14 @@ class PySimulation_API:
         if n:
             self._sim.run(n)
         st, ce = self._sim.spikes()
-        out = np.array([self._output_pop[q] for q in self._net.layer_of()[ce]], bool) if len(ce) else np.zeros(0, bool)
+        layer = self._net.layer_of()[ce] if len(ce) else np.zeros(0, np.int64)
+        if self._mon_spike_files:
+            mon = np.array([self._log_pop[q] for q in layer], bool)
+            lines = ["%f\t%d\n" % (self._sim.step_time(int(s)), int(c)) for s, c in zip(st[mon], ce[mon])]
+            for f in self._mon_spike_files:
+                with open(f, "a") as fh:
+                    fh.writelines(lines)
+        out = np.array([self._output_pop[q] for q in layer], bool)
         st, ce = st[out], ce[out]
         times = [self._sim.step_time(int(s)) for s in st]
         self._spikes_t.extend(times)

@@ -114,11 +114,19 @@ __device__ __forceinline__ void adex_deriv(const PopDev &P, const float *x, floa
 }
 
 // --------------------------------------------------------------------- HH --
+// Partial results of one HH derivative evaluation: the rates at V and the partial
+// sums of dV/dt, left to right as the reference adds them: s0 = current +
+// gl (eleak - V), a3 = gna m m m, sA = s0 + a3 h (ena - V), B = gkd n n n n (ek - V).
+struct HHParts {
+    float am, bm, ah, bh, an, bn;
+    float s0, a3, sA, B;
+};
+
 // p = e_exc e_inh e_leak g_leak c_m v_thr tau_exc tau_inh tau_nmda g_na g_kd e_na e_k
 // x = {V, m, h, n, gE, gI, gNMDA}.  The clamps write the state passed in, as the
 // reference does (HHTimeDrivenModel.cpp:197-222).
 template <int EN = -1>
-__device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
+__device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx, HHParts &R) {
     const int en = en_mask<EN>(P);
     const float *p = P.p;
     const float eexc = p[0], einh = p[1], eleak = p[2], gl = p[3], gna = p[9], gkd = p[10], ena = p[11], ek = p[12];
@@ -139,10 +147,62 @@ __device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
     if (en & 1) current += x[4] * (eexc - x[0]);
     if (en & 2) current += x[5] * (einh - x[0]);
     if (en & 4) current += x[6] * nmda_inf(P, x[0], einh) * (eexc - x[0]);
-    dx[0] = (current + gl * (eleak - V) + gna * m * m * m * h * (ena - V) + gkd * n * n * n * n * (ek - V)) * P.inv_c_m;
+    // (current + gl (eleak - V) + gna m m m h (ena - V) + gkd n n n n (ek - V)) / c_m
+    const float s0 = current + gl * (eleak - V);
+    const float a3 = gna * m * m * m;
+    const float sA = s0 + a3 * h * (ena - V);
+    const float B = gkd * n * n * n * n * (ek - V);
+    dx[0] = (sA + B) * P.inv_c_m;
     dx[1] = (am * (1.0f - m) - bm * m);
     dx[2] = (ah * (1.0f - h) - bh * h);
     dx[3] = (an * (1.0f - n) - bn * n);
+    R = HHParts{am, bm, ah, bh, an, bn, s0, a3, sA, B};
+}
+
+template <int EN = -1>
+__device__ __forceinline__ void hh_deriv(const PopDev &P, float *x, float *dx) {
+    HHParts R;
+    hh_deriv<EN>(P, x, dx, R);
+}
+
+// Columns m, h, n of the BDF Jacobian, (f(x) - f(x - eps e_j)) / eps, where x was
+// clamped by the evaluation that gave f(x) = fx and R.  Displacing one gate leaves
+// V, hence the rates, and the other gates' derivatives unchanged: their
+// differences are exactly zero, and dV/dt only needs its displaced term.  The
+// displaced gate is clamped as the full evaluation would clamp it, so every entry
+// is the full evaluation's bit for bit.
+__device__ __forceinline__ void hh_gate_columns(const PopDev &P, const float *x, const float *fx, const HHParts &R,
+                                                float eps, float inv_eps, float *jac) {
+    const float *p = P.p;
+    const float gna = p[9], gkd = p[10], ena = p[11], ek = p[12];
+    const float V = x[0], m = x[1], h = x[2], n = x[3];
+    float m2 = m - eps;
+    if (m2 < 0) m2 = 0.0f;
+    if (m2 > 1) m2 = 1.0f;
+    const float dm0 = (R.s0 + gna * m2 * m2 * m2 * h * (ena - V) + R.B) * P.inv_c_m;
+    const float dm1 = R.am * (1.0f - m2) - R.bm * m2;
+    float h2 = h - eps;
+    if (h2 < 0) h2 = 0.0f;
+    if (h2 > 1) h2 = 1.0f;
+    const float dh0 = (R.s0 + R.a3 * h2 * (ena - V) + R.B) * P.inv_c_m;
+    const float dh2 = R.ah * (1.0f - h2) - R.bh * h2;
+    float n2 = n - eps;
+    if (n2 < 0) n2 = 0.0f;
+    if ((double)n2 > 0.72) n2 = 0.72f;
+    const float dn0 = (R.sA + gkd * n2 * n2 * n2 * n2 * (ek - V)) * P.inv_c_m;
+    const float dn3 = R.an * (1.0f - n2) - R.bn * n2;
+    jac[0 * 4 + 1] = (fx[0] - dm0) * inv_eps;
+    jac[1 * 4 + 1] = (fx[1] - dm1) * inv_eps;
+    jac[2 * 4 + 1] = 0.0f;
+    jac[3 * 4 + 1] = 0.0f;
+    jac[0 * 4 + 2] = (fx[0] - dh0) * inv_eps;
+    jac[1 * 4 + 2] = 0.0f;
+    jac[2 * 4 + 2] = (fx[2] - dh2) * inv_eps;
+    jac[3 * 4 + 2] = 0.0f;
+    jac[0 * 4 + 3] = (fx[0] - dn0) * inv_eps;
+    jac[1 * 4 + 3] = 0.0f;
+    jac[2 * 4 + 3] = 0.0f;
+    jac[3 * 4 + 3] = (fx[3] - dn3) * inv_eps;
 }
 
 template <int KIND> struct Model;
@@ -305,8 +365,10 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
         int k = 0;
         const float eps_j = dt * 0.1f;
         const float inv_eps = 1.0f / eps_j;
+        HHParts R;
         while (epsi > 1e-6 && k < 10) {
-            M::template deriv<EN>(P, pr, aux, rf);
+            if constexpr (KIND == KIND_HH) hh_deriv<EN>(P, pr, aux, R);
+            else M::template deriv<EN>(P, pr, aux, rf);
 #pragma unroll
             for (int j = 0; j < ND; ++j) {
                 c[j] = co[0] * dt * aux[j] + co[1] * x[j];
@@ -316,7 +378,16 @@ __device__ __forceinline__ bool integrate(const PopDev &P, float *x, int refr, i
             // base point is f(pr), already in aux: deriv clamps its argument in
             // place before evaluating (HH) and clamping twice changes nothing, so
             // evaluating it again would give the same values bit for bit.
-            {
+            if constexpr (KIND == KIND_HH) {
+                float tmp[NV], neg[NV];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) tmp[v] = pr[v];
+                tmp[0] -= eps_j;
+                M::template deriv<EN>(P, tmp, neg, rf);
+#pragma unroll
+                for (int z = 0; z < ND; ++z) jac[z * ND] = (aux[z] - neg[z]) * inv_eps;
+                hh_gate_columns(P, pr, aux, R, eps_j, inv_eps, jac);
+            } else {
                 float tmp[NV], neg[NV];
                 const float *pos = aux;
 #pragma unroll

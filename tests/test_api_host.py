@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 
-def build_api():
+def build_api(log=False):
     import edlut_b200.api as pyedlut
     sim = pyedlut.PySimulation_API()
     inp = sim.AddNeuronLayer(num_neurons=3, model_name="InputSpikeNeuronModel", param_dict={},
@@ -15,7 +15,7 @@ def build_api():
     out = sim.AddNeuronLayer(num_neurons=2, model_name="LIFTimeDrivenModel",
                              param_dict={"v_thr": -50.0, "e_leak": -65.0, "g_leak": 0.2, "c_m": 2.0,
                                          "tau_ref": 1.0, "int_meth": im},
-                             log_activity=False, output_activity=True)
+                             log_activity=log, output_activity=True)
     rule = sim.AddLearningRule("STDP", {"max_LTP": 0.016, "tau_LTP": 0.010, "max_LTD": 0.033, "tau_LTD": 0.005})
     syn = sim.AddSynapticLayer([inp[0], inp[1], inp[2], out[0]], [out[0], out[1], out[1], out[1]],
                                {"weight": [6.0, 5.0, 5.0, 4.0], "max_weight": 10.0, "type": [0, 0, 1, 0],
@@ -76,3 +76,17 @@ def test_what_the_path_does_not_cover_raises():
         sim.AddExternalCurrentActivity([0.1], [0], [1.0])
     with pytest.raises(RuntimeError):
         sim.RunSimulation(0.01)
+
+
+def test_monitor_drivers_register_before_initialize(tmp_path):
+    """AddFileOutputMonitorDriver creates its file; one state file per simulation;
+    only layers added with log_activity (and not input layers) are monitored."""
+    sim, inp, out, rule, syn = build_api(log=True)
+    f1, f2, f3 = (str(tmp_path / n) for n in ("s.txt", "p.txt", "q.txt"))
+    sim.AddFileOutputMonitorDriver(f1, True)
+    sim.AddFileOutputMonitorDriver(f2, False)
+    assert open(f1).read() == "" and open(f2).read() == ""
+    with pytest.raises(NotImplementedError):
+        sim.AddFileOutputMonitorDriver(f3, True)
+    assert sim._log_pop == [False, True]
+    assert [l.log for l in sim._net.layers] == [0, 1]

@@ -39,3 +39,40 @@ def test_python_interface_run_matches_the_oracle(oracle, tmp_path):
     np.testing.assert_array_equal(np.float32(sim.GetWeights()), r["w_final"].astype(np.float32))
     n_eq, vals = sim.GetCompressedWeights()
     assert sum(n_eq) == len(syn)
+
+
+def test_python_interface_monitor_drivers(oracle, tmp_path):
+    """AddFileOutputMonitorDriver through RunSimulation slots: the spike monitor
+    holds the monitored layer's spikes in the -of format, and the state monitor is
+    the file one device run of the same network writes (the format the reference
+    files pin)."""
+    from edlut_b200.network import poisson_input_times
+    from edlut_b200.simulation import Simulation
+    from tests.test_api_host import build_api
+    sim, inp, out, rule, syn = build_api(log=True)
+    sf, pf = str(tmp_path / "states.txt"), str(tmp_path / "spikes.txt")
+    sim.AddFileOutputMonitorDriver(sf, True)
+    sim.AddFileOutputMonitorDriver(pf, False)
+    t, c = poisson_input_times(np.random.default_rng(4), 3, 80.0, 0.1)
+    sim.AddExternalSpikeActivity(t.astype(np.float64).tolist(), (c + inp[0]).tolist())
+    sim.Initialize()
+    for k in range(1, 11):
+        sim.RunSimulation(0.01 * k)
+    nsteps = sim._sim.counters()["steps"]
+    r = oracle.run(sim._net, t, c + inp[0], nsteps)
+    keep = np.isin(r["spike_cell"], out)
+    ref = spike_pairs(r["spike_step"][keep], r["spike_cell"][keep])
+    assert len(ref) > 5
+    ts = oracle.step_times(1e-4, nsteps)
+    assert open(pf).read() == "".join("%f\t%d\n" % (ts[s], cl) for s, cl in ref.tolist())
+    one = Simulation.from_description(sim._net)
+    one.inject_spikes(t, c + inp[0])
+    f1 = str(tmp_path / "one.txt")
+    one.open_monitor(f1)
+    one.run(nsteps)
+    one.close_monitor()
+    one.close()
+    sim._sim.close_monitor()
+    got = open(sf).read()
+    assert got == open(f1).read()
+    assert got.count("\n") >= 2 * nsteps
