@@ -524,10 +524,13 @@ __global__ void __launch_bounds__(kNarrowTile, narrow_min_blocks(KIND, INTEG)) k
 // at its position; one thread per conductance then adds the weights in delivery
 // order.  Up to kWideSmem arrivals: bitonic sort in shared memory; beyond, a
 // serial insertion sort in global memory.
+// A 512-arrival stage keeps a block at about 70 KB of shared memory, so three
+// fit an SM (85 registers a thread): the wide population packs onto fewer SMs
+// and leaves the others whole to the thread-per-neuron populations.
 constexpr int kWideThreads = 256;
 constexpr int kWideSmem = 1024;
 constexpr int kRankSort = 256;
-static_assert(kRankSort <= kWideThreads && kWideThreads == kNarrowTile, "wide blocks rank with one thread per arrival");
+static_assert(kRankSort <= kWideThreads && kWideThreads <= kNarrowTile, "wide blocks rank with one thread per arrival");
 
 // Steps of one launch (the runtime's window length).
 constexpr int kMaxWindow = 8;
@@ -850,8 +853,8 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
 // delivers on two steps runs its steps serially on warp 0 over one staged record
 // per synapse; a step with more arrivals than the stage holds runs on the
 // per-step path (wide_step).
-constexpr int kStage = 1024;          // arrivals of one chunk
-constexpr int kStageHashBits = 11;    // open-addressing table of the chunk's synapses
+constexpr int kStage = 512;           // arrivals of one chunk
+constexpr int kStageHashBits = 10;    // open-addressing table of the chunk's synapses
 constexpr int kStageHash = 1 << kStageHashBits;
 constexpr uint32_t kHashEmpty = 0xffffffffu;
 static_assert(kStage <= kWideSmem, "a staged chunk's weights fit the fold buffer");
@@ -1123,10 +1126,9 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
 
 // Steps k .. k+nsteps-1 of the block's neurons (spike list as in k_update_narrow).
 // Populations whose synapses cannot deliver twice in one step take the staged
-// window; the others run step by step.  Two blocks per SM (the staging area allows
-// two): up to 128 registers, so the serial per-step code runs without spills.
+// window; the others run step by step.  Three blocks per SM (85 registers).
 template <int KIND, int INTEG>
-__global__ void __launch_bounds__(kWideThreads, 2) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
+__global__ void __launch_bounds__(kWideThreads, 3) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
                                                                  double push_inv_dt) {
     __shared__ WideSmem S;
     extern __shared__ __align__(32) unsigned char stage_raw[];
