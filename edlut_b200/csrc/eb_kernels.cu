@@ -184,6 +184,13 @@ __device__ __forceinline__ void monitor_delivery(const PopDev &P, const NetDev &
     }
 }
 
+// Monitor hooks: MON 0 compiles them out, 1 keeps them on, 2 asks P.mon at run
+// time (the persistent kernel).  The hot kernels are instantiated with 0 and 1:
+// a run-time test in the thread-per-neuron update cost the stiff HH network
+// 70 % of its step.
+template <int MON>
+__device__ __forceinline__ bool mon_on(const PopDev &P) { return MON == 1 || (MON == 2 && P.mon != 0); }
+
 template <int ND>
 __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
     if (ty == 0) x[ND] += w;
@@ -193,14 +200,14 @@ __device__ __forceinline__ void add_conductance(float *x, int ty, float w) {
 
 // Apply one arrival at neuron i: g[type] += w (weight before plasticity), then
 // STDP pre (after the target's deferred post updates, when it keeps a ring).
-template <int ND>
+template <int ND, int MON = 2>
 __device__ __forceinline__ void apply_arrival(const PopDev &P, const NetDev &N, int64_t k, int64_t i, const Arrival &r,
                                               float *x) {
     const uint32_t tp = r.tpos;
     SynRec s = N.syn[tp];
     if (s.rule >= 0 && P.post_t) apply_pending_post(P, N, i, s);
     add_conductance<ND>(x, s.stype, s.w);
-    if (P.mon) monitor_delivery(P, N, k, i, r, s.stype, s.w);
+    if (mon_on<MON>(P)) monitor_delivery(P, N, k, i, r, s.stype, s.w);
     if (s.rule >= 0) stdp_pre(N, tp, s, r.a);
 }
 
@@ -403,7 +410,7 @@ constexpr int kNarrowTile = 256;
 
 // One step of neuron i (lanes with active unset only join the warp collectives);
 // x and ax hold its state, loaded and stored by the caller.
-template <int KIND, int INTEG, int EN = -1>
+template <int KIND, int INTEG, int EN = -1, int MON = 2>
 __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, int64_t k, int64_t i, bool active,
                                             float *x, NeuronAux &ax, bool list, double push_inv_dt) {
     constexpr int ND = Model<KIND>::ND;
@@ -420,7 +427,7 @@ __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, in
             if (c > capg) { atomicOr(N.flags, FLAG_BUCKET_OVERFLOW); c = capg; }
             Arrival *r = N.rec + (int64_t)slot * N.cap_total + N.cap_base[gi];
             if (c == 1) {
-                apply_arrival<ND>(P, N, k, i, r[0], x);
+                apply_arrival<ND, MON>(P, N, k, i, r[0], x);
             } else if (c <= kLocalSort) {
                 Arrival loc[kLocalSort];
                 for (uint32_t a = 0; a < c; ++a) {
@@ -429,7 +436,7 @@ __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, in
                     while (b >= 0 && arr_less(v, loc[b])) { loc[b + 1] = loc[b]; --b; }
                     loc[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, loc[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND, MON>(P, N, k, i, loc[a], x);
             } else {
                 for (uint32_t a = 1; a < c; ++a) {  // in-place insertion sort (rare path)
                     Arrival v = r[a];
@@ -437,12 +444,12 @@ __device__ __forceinline__ void narrow_step(const PopDev &P, const NetDev &N, in
                     while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
                     r[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, r[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND, MON>(P, N, k, i, r[a], x);
             }
         }
         sp = advance_neuron<KIND, INTEG, EN>(P, N, i, x, ax);
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
-        if (P.mon) monitor_state(P, N, k, i, x, Model<KIND>::NV, sp);
+        if (mon_on<MON>(P)) monitor_state(P, N, k, i, x, Model<KIND>::NV, sp);
         if (sp && P.post_t) note_post_spike(P, N, i, k);
     }
     // delivered-event counter: one atomic per warp
@@ -489,7 +496,7 @@ constexpr int narrow_min_blocks(int kind, int integ) {
     return (kind == KIND_HH && integ == INTEG_BDF) ? 3 : (kind != KIND_HH && integ != INTEG_BDF) ? 6 : 0;
 }
 
-template <int KIND, int INTEG, int EN>
+template <int KIND, int INTEG, int EN, int MON>
 __global__ void __launch_bounds__(kNarrowTile, narrow_min_blocks(KIND, INTEG)) k_update_narrow(PopDev P, NetDev N, int rel, int nsteps,
                                                                 double push_inv_dt) {
     const int64_t k = cur_step(N, rel);
@@ -503,7 +510,7 @@ __global__ void __launch_bounds__(kNarrowTile, narrow_min_blocks(KIND, INTEG)) k
         load_state<KIND>(P, i, x);
         ax = load_aux<KIND, INTEG>(P, i);
     }
-    for (int s = 0; s < nsteps; ++s) narrow_step<KIND, INTEG, EN>(P, N, k + s, i, active, x, ax, list, push_inv_dt);
+    for (int s = 0; s < nsteps; ++s) narrow_step<KIND, INTEG, EN, MON>(P, N, k + s, i, active, x, ax, list, push_inv_dt);
     if (active) {
         store_state<KIND>(P, i, x);
         store_aux<KIND, INTEG>(P, i, ax);
@@ -634,7 +641,7 @@ __device__ __forceinline__ void wide_fold(WideSmem &S, float *x, uint32_t c) {
 
 // One step of wide neuron i by the whole block; thread 0 holds its state in x and
 // ax (loaded and stored by the caller).
-template <int KIND, int INTEG>
+template <int KIND, int INTEG, int MON = 2>
 // pf_n: records of this step already copied to S.next_rec (with the count in
 // S.next_c; 0: none), updated for the next step when has_next (the next step is
 // in the same launch).
@@ -713,7 +720,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                 if (own) S.sbuf[S.rank[tid]] = v;
                 __syncthreads();
                 if (tid == 0)
-                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, S.sbuf[a], x);
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND, MON>(P, N, k, i, S.sbuf[a], x);
             } else {
                 if (own) {
                     if (rec.rule >= 0) {
@@ -724,7 +731,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                         S.sw[S.rank[tid]] = rec.w;
                     }
                     S.sty[S.rank[tid]] = rec.stype;
-                    if (P.mon) monitor_delivery(P, N, k, i, v, rec.stype, S.sw[S.rank[tid]]);
+                    if (mon_on<MON>(P)) monitor_delivery(P, N, k, i, v, rec.stype, S.sw[S.rank[tid]]);
                 }
                 wide_fold<ND>(S, x, c);
             }
@@ -752,7 +759,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                 }
             if (P.may_repeat) {
                 if (tid == 0)
-                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, S.sbuf[a], x);
+                    for (uint32_t a = 0; a < c; ++a) apply_arrival<ND, MON>(P, N, k, i, S.sbuf[a], x);
             } else {
                 for (int a = tid; a < (int)c; a += nt) {
                     const Arrival v = S.sbuf[a];
@@ -761,7 +768,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                     stdp_pre_gather(P, N, i, v.tpos, v.a, w_old, ty);
                     S.sw[a] = w_old;
                     S.sty[a] = (uint8_t)ty;
-                    if (P.mon) monitor_delivery(P, N, k, i, v, ty, w_old);
+                    if (mon_on<MON>(P)) monitor_delivery(P, N, k, i, v, ty, w_old);
                 }
                 __syncthreads();
                 wide_fold<ND>(S, x, c);
@@ -777,7 +784,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
                     while (b >= 0 && arr_less(v, r[b])) { r[b + 1] = r[b]; --b; }
                     r[b + 1] = v;
                 }
-                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND>(P, N, k, i, r[a], x);
+                for (uint32_t a = 0; a < c; ++a) apply_arrival<ND, MON>(P, N, k, i, r[a], x);
             }
         }
         if (tid == 0) atomicAdd(P.events, (unsigned long long)c);
@@ -798,7 +805,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
             }
         }
         record_trace(P, N, k, gi, x, Model<KIND>::NV);
-        if (P.mon) monitor_state(P, N, k, i, x, Model<KIND>::NV, sp);
+        if (mon_on<MON>(P)) monitor_state(P, N, k, i, x, Model<KIND>::NV, sp);
         if (sp) {
             if (list) {
                 const uint32_t o = atomicAdd(&P.spk_count[k & 1], 1u);
@@ -929,7 +936,7 @@ __device__ __forceinline__ void ordered_sum(const WideSmem &S, uint32_t o0, uint
 // Lane 0 of warp 0, after step ks's conductances are in x: integrate, test the
 // spike, note it for deferred post-synaptic STDP (global ring and its staged
 // copy), trace, spike list and recording.  Returns the spike flag.
-template <int KIND, int INTEG>
+template <int KIND, int INTEG, int MON = 2>
 __device__ __forceinline__ int wide_advance(const PopDev &P, const NetDev &N, int64_t ks, int64_t i, WideSmem &S,
                                             float *x, NeuronAux &ax, bool list, bool ring) {
     const int64_t gi = P.first + i;
@@ -942,7 +949,7 @@ __device__ __forceinline__ int wide_advance(const PopDev &P, const NetDev &N, in
         if (P.post_f) S.ring_f[q] = P.post_f[i * kPostRing + q];
     }
     record_trace(P, N, ks, gi, x, Model<KIND>::NV);
-    if (P.mon) monitor_state(P, N, ks, i, x, Model<KIND>::NV, sp != 0);
+    if (mon_on<MON>(P)) monitor_state(P, N, ks, i, x, Model<KIND>::NV, sp != 0);
     if (sp) {
         if (list) {
             const uint32_t o = atomicAdd(&P.spk_count[ks & 1], 1u);
@@ -959,7 +966,7 @@ __device__ __forceinline__ int wide_advance(const PopDev &P, const NetDev &N, in
     return sp;
 }
 
-template <int KIND, int INTEG>
+template <int KIND, int INTEG, int MON = 2>
 __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
                                             StageSmem &G, float *x, NeuronAux &ax, int nsteps, bool list,
                                             double push_inv_dt) {
@@ -995,7 +1002,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
         while (s1 < nsteps && S.woff[s1 + 1] - S.woff[s0] <= (uint32_t)kStage) ++s1;
         if (s1 == s0) {  // this step alone overflows the stage
             int pf_n = 0;
-            wide_step<KIND, INTEG>(P, N, k + s0, i, S, x, ax, list, push_inv_dt, pf_n, false);
+            wide_step<KIND, INTEG, MON>(P, N, k + s0, i, S, x, ax, list, push_inv_dt, pf_n, false);
             __syncthreads();
             ++s0;
             continue;
@@ -1060,7 +1067,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                     const uint32_t pos = S.woff[stage_step_of(S, s0, a0 + a)] - a0 + G.rank[a];
                     S.sw[pos] = r.w;
                     S.sty[pos] = r.stype;
-                    if (P.mon) monitor_delivery(P, N, k + stage_step_of(S, s0, a0 + a), i, G.arr[a], r.stype, r.w);
+                    if (mon_on<MON>(P)) monitor_delivery(P, N, k + stage_step_of(S, s0, a0 + a), i, G.arr[a], r.stype, r.w);
                     if (r.rule >= 0) stdp_pre_rec(N, r, G.arr[a].a);
                     G.rec[a] = r;
                 }
@@ -1071,7 +1078,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                         int sp = 0;
                         if (lane == 0) {
                             ordered_sum<ND>(S, S.woff[j] - a0, S.wcnt[j], x, P.en);
-                            sp = wide_advance<KIND, INTEG>(P, N, k + j, i, S, x, ax, list, ring);
+                            sp = wide_advance<KIND, INTEG, MON>(P, N, k + j, i, S, x, ax, list, ring);
                         }
                         sp = __shfl_sync(0xffffffffu, sp, 0);
                         if (sp && push_inv_dt > 0.0) push_from(P, N, k + j, gi, lane, 32, push_inv_dt);
@@ -1092,7 +1099,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                     if (r.rule >= 0 && ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, prule, r);
                     S.sw[o0 + G.rank[a]] = r.w;
                     S.sty[o0 + G.rank[a]] = r.stype;
-                    if (P.mon) monitor_delivery(P, N, ks, i, G.arr[a], r.stype, r.w);
+                    if (mon_on<MON>(P)) monitor_delivery(P, N, ks, i, G.arr[a], r.stype, r.w);
                     if (r.rule >= 0) {
                         stdp_pre_rec(N, r, G.arr[a].a);
                         sr = r;
@@ -1102,7 +1109,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                 int sp = 0;
                 if (lane == 0) {
                     ordered_sum<ND>(S, o0, c, x, P.en);
-                    sp = wide_advance<KIND, INTEG>(P, N, ks, i, S, x, ax, list, ring);
+                    sp = wide_advance<KIND, INTEG, MON>(P, N, ks, i, S, x, ax, list, ring);
                 }
                 sp = __shfl_sync(0xffffffffu, sp, 0);
                 if (sp && push_inv_dt > 0.0) push_from(P, N, ks, gi, lane, 32, push_inv_dt);
@@ -1127,7 +1134,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
 // Steps k .. k+nsteps-1 of the block's neurons (spike list as in k_update_narrow).
 // Populations whose synapses cannot deliver twice in one step take the staged
 // window; the others run step by step.  Three blocks per SM (85 registers).
-template <int KIND, int INTEG>
+template <int KIND, int INTEG, int MON>
 __global__ void __launch_bounds__(kWideThreads, 3) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
                                                                  double push_inv_dt) {
     __shared__ WideSmem S;
@@ -1146,11 +1153,11 @@ __global__ void __launch_bounds__(kWideThreads, 3) k_update_wide(PopDev P, NetDe
         }
         __syncthreads();  // S.ring_ok reset before any thread reads it
         if (!P.may_repeat && nsteps <= kMaxWindow) {
-            wide_window<KIND, INTEG>(P, N, k, i, S, G, x, ax, nsteps, list, push_inv_dt);
+            wide_window<KIND, INTEG, MON>(P, N, k, i, S, G, x, ax, nsteps, list, push_inv_dt);
         } else {
             int pf_n = 0;
             for (int s = 0; s < nsteps; ++s)
-                wide_step<KIND, INTEG>(P, N, k + s, i, S, x, ax, list, push_inv_dt, pf_n, s + 1 < nsteps);
+                wide_step<KIND, INTEG, MON>(P, N, k + s, i, S, x, ax, list, push_inv_dt, pf_n, s + 1 < nsteps);
         }
         if (threadIdx.x == 0) {
             store_state<KIND>(P, i, x);
@@ -1519,13 +1526,16 @@ template <int KIND, int INTEG>
 static void launch_update_t(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st) {
     if (P.wide) {
         const int blocks = (int)std::min<int64_t>(P.n, 148 * 8);
-        k_update_wide<KIND, INTEG><<<blocks, kWideThreads, stage_smem_bytes(), st>>>(P, N, rel, nsteps, push_inv_dt);
+        if (P.mon) k_update_wide<KIND, INTEG, 1><<<blocks, kWideThreads, stage_smem_bytes(), st>>>(P, N, rel, nsteps, push_inv_dt);
+        else k_update_wide<KIND, INTEG, 0><<<blocks, kWideThreads, stage_smem_bytes(), st>>>(P, N, rel, nsteps, push_inv_dt);
     } else {
-        // the common conductance sets get kernels with the set compiled in
+        // the common conductance sets get kernels with the set compiled in; a
+        // monitored population takes the generic kernel with the monitor hooks
         const int blocks = (int)((P.n + 255) / 256);
-        if (P.en == 1) k_update_narrow<KIND, INTEG, 1><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
-        else if (P.en == 3) k_update_narrow<KIND, INTEG, 3><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
-        else k_update_narrow<KIND, INTEG, -1><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        if (P.mon) k_update_narrow<KIND, INTEG, -1, 1><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        else if (P.en == 1) k_update_narrow<KIND, INTEG, 1, 0><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        else if (P.en == 3) k_update_narrow<KIND, INTEG, 3, 0><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
+        else k_update_narrow<KIND, INTEG, -1, 0><<<blocks, 256, 0, st>>>(P, N, rel, nsteps, push_inv_dt);
     }
 }
 
@@ -1542,10 +1552,14 @@ static void launch_update_k(const PopDev &P, const NetDev &N, int rel, int nstep
 template <int KIND>
 static cudaError_t prepare_wide_k() {
     const int bytes = (int)stage_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;
 }
 
