@@ -641,7 +641,7 @@ __device__ __forceinline__ void wide_fold(WideSmem &S, float *x, uint32_t c) {
 
 // One step of wide neuron i by the whole block; thread 0 holds its state in x and
 // ax (loaded and stored by the caller).
-template <int KIND, int INTEG, int MON = 2>
+template <int KIND, int INTEG, int MON = 2, int EN = -1>
 // pf_n: records of this step already copied to S.next_rec (with the count in
 // S.next_c; 0: none), updated for the next step when has_next (the next step is
 // in the same launch).
@@ -793,7 +793,7 @@ __device__ __forceinline__ void wide_step(const PopDev &P, const NetDev &N, int6
         issue_next();
     }
     if (tid == 0) {
-        const bool sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax);
+        const bool sp = advance_neuron<KIND, INTEG, EN>(P, N, i, x, ax);
         S.spiked = sp ? 1 : 0;
         if (sp && P.post_t) {
             note_post_spike(P, N, i, k);
@@ -936,11 +936,11 @@ __device__ __forceinline__ void ordered_sum(const WideSmem &S, uint32_t o0, uint
 // Lane 0 of warp 0, after step ks's conductances are in x: integrate, test the
 // spike, note it for deferred post-synaptic STDP (global ring and its staged
 // copy), trace, spike list and recording.  Returns the spike flag.
-template <int KIND, int INTEG, int MON = 2>
+template <int KIND, int INTEG, int MON = 2, int EN = -1>
 __device__ __forceinline__ int wide_advance(const PopDev &P, const NetDev &N, int64_t ks, int64_t i, WideSmem &S,
                                             float *x, NeuronAux &ax, bool list, bool ring) {
     const int64_t gi = P.first + i;
-    const int sp = advance_neuron<KIND, INTEG>(P, N, i, x, ax) ? 1 : 0;
+    const int sp = advance_neuron<KIND, INTEG, EN>(P, N, i, x, ax) ? 1 : 0;
     if (sp && ring) {
         note_post_spike(P, N, i, ks);
         const uint32_t n1 = P.post_n[i], q = (n1 - 1) % kPostRing;
@@ -966,7 +966,7 @@ __device__ __forceinline__ int wide_advance(const PopDev &P, const NetDev &N, in
     return sp;
 }
 
-template <int KIND, int INTEG, int MON = 2>
+template <int KIND, int INTEG, int MON = 2, int EN = -1>
 __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, int64_t k, int64_t i, WideSmem &S,
                                             StageSmem &G, float *x, NeuronAux &ax, int nsteps, bool list,
                                             double push_inv_dt) {
@@ -1002,7 +1002,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
         while (s1 < nsteps && S.woff[s1 + 1] - S.woff[s0] <= (uint32_t)kStage) ++s1;
         if (s1 == s0) {  // this step alone overflows the stage
             int pf_n = 0;
-            wide_step<KIND, INTEG, MON>(P, N, k + s0, i, S, x, ax, list, push_inv_dt, pf_n, false);
+            wide_step<KIND, INTEG, MON, EN>(P, N, k + s0, i, S, x, ax, list, push_inv_dt, pf_n, false);
             __syncthreads();
             ++s0;
             continue;
@@ -1077,8 +1077,8 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                     for (int j = s; j < s1; ++j) {
                         int sp = 0;
                         if (lane == 0) {
-                            ordered_sum<ND>(S, S.woff[j] - a0, S.wcnt[j], x, P.en);
-                            sp = wide_advance<KIND, INTEG, MON>(P, N, k + j, i, S, x, ax, list, ring);
+                            ordered_sum<ND>(S, S.woff[j] - a0, S.wcnt[j], x, en_mask<EN>(P));
+                            sp = wide_advance<KIND, INTEG, MON, EN>(P, N, k + j, i, S, x, ax, list, ring);
                         }
                         sp = __shfl_sync(0xffffffffu, sp, 0);
                         if (sp && push_inv_dt > 0.0) push_from(P, N, k + j, gi, lane, 32, push_inv_dt);
@@ -1108,8 +1108,8 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                 __syncwarp();
                 int sp = 0;
                 if (lane == 0) {
-                    ordered_sum<ND>(S, o0, c, x, P.en);
-                    sp = wide_advance<KIND, INTEG, MON>(P, N, ks, i, S, x, ax, list, ring);
+                    ordered_sum<ND>(S, o0, c, x, en_mask<EN>(P));
+                    sp = wide_advance<KIND, INTEG, MON, EN>(P, N, ks, i, S, x, ax, list, ring);
                 }
                 sp = __shfl_sync(0xffffffffu, sp, 0);
                 if (sp && push_inv_dt > 0.0) push_from(P, N, ks, gi, lane, 32, push_inv_dt);
@@ -1134,7 +1134,7 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
 // Steps k .. k+nsteps-1 of the block's neurons (spike list as in k_update_narrow).
 // Populations whose synapses cannot deliver twice in one step take the staged
 // window; the others run step by step.  Three blocks per SM (85 registers).
-template <int KIND, int INTEG, int MON>
+template <int KIND, int INTEG, int MON, int EN>
 __global__ void __launch_bounds__(kWideThreads, 3) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
                                                                  double push_inv_dt) {
     __shared__ WideSmem S;
@@ -1153,11 +1153,11 @@ __global__ void __launch_bounds__(kWideThreads, 3) k_update_wide(PopDev P, NetDe
         }
         __syncthreads();  // S.ring_ok reset before any thread reads it
         if (!P.may_repeat && nsteps <= kMaxWindow) {
-            wide_window<KIND, INTEG, MON>(P, N, k, i, S, G, x, ax, nsteps, list, push_inv_dt);
+            wide_window<KIND, INTEG, MON, EN>(P, N, k, i, S, G, x, ax, nsteps, list, push_inv_dt);
         } else {
             int pf_n = 0;
             for (int s = 0; s < nsteps; ++s)
-                wide_step<KIND, INTEG, MON>(P, N, k + s, i, S, x, ax, list, push_inv_dt, pf_n, s + 1 < nsteps);
+                wide_step<KIND, INTEG, MON, EN>(P, N, k + s, i, S, x, ax, list, push_inv_dt, pf_n, s + 1 < nsteps);
         }
         if (threadIdx.x == 0) {
             store_state<KIND>(P, i, x);
@@ -1526,8 +1526,10 @@ template <int KIND, int INTEG>
 static void launch_update_t(const PopDev &P, const NetDev &N, int rel, int nsteps, double push_inv_dt, cudaStream_t st) {
     if (P.wide) {
         const int blocks = (int)std::min<int64_t>(P.n, 148 * 8);
-        if (P.mon) k_update_wide<KIND, INTEG, 1><<<blocks, kWideThreads, stage_smem_bytes(), st>>>(P, N, rel, nsteps, push_inv_dt);
-        else k_update_wide<KIND, INTEG, 0><<<blocks, kWideThreads, stage_smem_bytes(), st>>>(P, N, rel, nsteps, push_inv_dt);
+        const size_t sm = stage_smem_bytes();
+        if (P.mon) k_update_wide<KIND, INTEG, 1, -1><<<blocks, kWideThreads, sm, st>>>(P, N, rel, nsteps, push_inv_dt);
+        else if (P.en == 1) k_update_wide<KIND, INTEG, 0, 1><<<blocks, kWideThreads, sm, st>>>(P, N, rel, nsteps, push_inv_dt);
+        else k_update_wide<KIND, INTEG, 0, -1><<<blocks, kWideThreads, sm, st>>>(P, N, rel, nsteps, push_inv_dt);
     } else {
         // the common conductance sets get kernels with the set compiled in; a
         // monitored population takes the generic kernel with the monitor hooks
@@ -1552,14 +1554,18 @@ static void launch_update_k(const PopDev &P, const NetDev &N, int rel, int nstep
 template <int KIND>
 static cudaError_t prepare_wide_k() {
     const int bytes = (int)stage_smem_bytes();
-    cudaError_t e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaError_t e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER, 0, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_EULER, 1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2, 0, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK2, 1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4, 0, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_RK4, 1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF, 0, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF, 0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_update_wide<KIND, INTEG_BDF, 1, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     return e;
 }
 
