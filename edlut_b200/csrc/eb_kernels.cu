@@ -550,6 +550,8 @@ struct WideSmem {
     float g[3];                         // conductances handed to the per-type adders
     uint32_t wcnt[kMaxWindow];          // staged window: arrivals of each step
     uint32_t woff[kMaxWindow + 1];      // and their offsets (exclusive scan)
+    unsigned long long kmin[kMaxWindow];  // smallest and largest time key of each step's arrivals
+    unsigned long long kmax[kMaxWindow];
     int dup;                            // a synapse of the staged chunk delivers twice
     int next_s;                         // first step of the chunk's next round
     unsigned long long khi[kRankSort];  // arrival time keys
@@ -995,6 +997,10 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
         for (int s = 0; s < nsteps; ++s) S.woff[s + 1] = S.woff[s] + S.wcnt[s];
         if (ring) S.ring_ok = 1;
     }
+    if (tid < nsteps) {
+        S.kmin[tid] = ~0ull;
+        S.kmax[tid] = 0ull;
+    }
     __syncthreads();
     int s0 = 0;
     while (s0 < nsteps) {
@@ -1013,8 +1019,16 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
             const int slot = (int)((k + s) & (N.R - 1));
             const Arrival v = N.rec[(int64_t)slot * N.cap_total + rbase + (a0 + a - S.woff[s])];
             G.arr[a] = v;
-            G.key[a] = time_key(v.a);
+            const unsigned long long key = time_key(v.a);
+            G.key[a] = key;
+            atomicMin(&S.kmin[s], key);
+            atomicMax(&S.kmax[s], key);
+            // the synapse record, copied while the chunk is hashed and ranked
+            const SynRec *src = N.syn + v.tpos;
+            cp_async16(&G.rec[a], src);
+            cp_async16(reinterpret_cast<unsigned char *>(&G.rec[a]) + 16, reinterpret_cast<const unsigned char *>(src) + 16);
         }
+        cp_async_commit();
         for (int h = tid; h < kStageHash; h += nt) G.hkey[h] = kHashEmpty;
         if (tid == 0) S.dup = 0;
         __syncthreads();
@@ -1031,9 +1045,15 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
                 h = (h + 1) & (kStageHash - 1);
             }
             G.own[a] = (uint16_t)h;
+            // a step whose arrival times span less than 2^32 key units ranks on
+            // one 64-bit key: (time key - the step's smallest) << 32 | synapse order
+            const int s = stage_step_of(S, s0, a0 + a);
+            const unsigned long long k0 = S.kmin[s];
+            if (S.kmax[s] - k0 <= 0xffffffffull) G.key[a] = ((G.key[a] - k0) << 32) | G.arr[a].spos;
         }
         __syncthreads();
         const bool dup = S.dup != 0;
+        if (dup) cp_async_wait_all();  // the serial path below rewrites staged records
         for (uint32_t a = tid; a < T; a += nt) {
             const uint32_t o = G.hval[G.own[a]];
             G.own[a] = (uint16_t)o;
@@ -1048,21 +1068,29 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
             const int s = stage_step_of(S, s0, a0 + a);
             const uint32_t b0 = S.woff[s] - a0, b1 = S.woff[s + 1] - a0;
             const unsigned long long ka = G.key[a];
-            const uint32_t pa = G.arr[a].spos;
             uint32_t r = 0;
+            if (S.kmax[s] - S.kmin[s] <= 0xffffffffull) {
+#pragma unroll 8
+                for (uint32_t b = b0; b < b1; ++b) r += G.key[b] < ka ? 1u : 0u;
+            } else {
+                const uint32_t pa = G.arr[a].spos;
 #pragma unroll 4
-            for (uint32_t b = b0; b < b1; ++b) {
-                const unsigned long long kb = G.key[b];
-                r += (kb < ka || (kb == ka && G.arr[b].spos < pa)) ? 1u : 0u;
+                for (uint32_t b = b0; b < b1; ++b) {
+                    const unsigned long long kb = G.key[b];
+                    r += (kb < ka || (kb == ka && G.arr[b].spos < pa)) ? 1u : 0u;
+                }
             }
             G.rank[a] = (uint16_t)r;
         }
+        cp_async_wait_all();
         __syncthreads();
         if (!dup) {
             int s = s0;
             while (s < s1) {
                 for (uint32_t a = S.woff[s] - a0 + tid; a < T; a += nt) {
-                    SynRec r = N.syn[G.arr[a].tpos];
+                    // the first round reads the staged copy; later ones the record in
+                    // global memory, untouched until the chunk writes back
+                    SynRec r = s == s0 ? G.rec[a] : N.syn[G.arr[a].tpos];
                     if (r.rule >= 0 && ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, prule, r);
                     const uint32_t pos = S.woff[stage_step_of(S, s0, a0 + a)] - a0 + G.rank[a];
                     S.sw[pos] = r.w;
