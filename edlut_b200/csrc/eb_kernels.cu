@@ -854,11 +854,11 @@ __device__ __forceinline__ void update_wide_neuron(const PopDev &P, const NetDev
 // step.  When every synapse of the chunk delivers once (the usual case), the
 // chunk's steps run in rounds: the whole block computes, in parallel, every
 // remaining arrival's synapse update -- deferred post-synaptic catch-up on the
-// target's spikes so far, the delivered weight at its position, the STDP pre
-// update -- then warp 0 runs the steps in order (ordered sums, integration, spike,
-// fan-out) until the neuron spikes.  A spike changes the catch-up of the later
-// arrivals, so the next round recomputes those from their records in global
-// memory, untouched until the chunk writes back.  A chunk in which a synapse
+// target's spikes so far and the delivered weight at its position -- then warp 0
+// runs the steps in order (ordered sums, integration, spike, fan-out) until the
+// neuron spikes.  A spike adds one update to the catch-up of the later arrivals:
+// the next round applies it to their staged records.  The STDP pre updates are
+// applied as the chunk writes its records back.  A chunk in which a synapse
 // delivers on two steps runs its steps serially on warp 0 over one staged record
 // per synapse; a step with more arrivals than the stage holds runs on the
 // per-step path (wide_step).
@@ -1088,15 +1088,16 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
             int s = s0;
             while (s < s1) {
                 for (uint32_t a = S.woff[s] - a0 + tid; a < T; a += nt) {
-                    // the first round reads the staged copy; later ones the record in
-                    // global memory, untouched until the chunk writes back
-                    SynRec r = s == s0 ? G.rec[a] : N.syn[G.arr[a].tpos];
+                    // the staged record, caught up to the spikes of the earlier rounds:
+                    // this round adds the spike that ended the last one (the same
+                    // updates in the same order as one catch-up from the original);
+                    // the pre-synaptic update is applied at the write-back
+                    SynRec r = G.rec[a];
                     if (r.rule >= 0 && ring) apply_pending(N, RingSmem{S.ring, S.ring_f}, S.ring_n, prule, r);
                     const uint32_t pos = S.woff[stage_step_of(S, s0, a0 + a)] - a0 + G.rank[a];
                     S.sw[pos] = r.w;
                     S.sty[pos] = r.stype;
                     if (mon_on<MON>(P)) monitor_delivery(P, N, k + stage_step_of(S, s0, a0 + a), i, G.arr[a], r.stype, r.w);
-                    if (r.rule >= 0) stdp_pre_rec(N, r, G.arr[a].a);
                     G.rec[a] = r;
                 }
                 __syncthreads();
@@ -1147,7 +1148,8 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
         __syncthreads();
         for (uint32_t a = tid; a < T; a += nt) {
             if (G.own[a] != a || G.rec[a].rule < 0) continue;
-            const SynRec &r = G.rec[a];
+            SynRec r = G.rec[a];
+            if (!dup) stdp_pre_rec(N, r, G.arr[a].a);  // the serial path applied it already
             SynRec *d = N.syn + G.arr[a].tpos;
             d->w = r.w;
             d->pre = r.pre;
