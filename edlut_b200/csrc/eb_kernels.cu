@@ -1163,9 +1163,10 @@ __device__ __forceinline__ void wide_window(const PopDev &P, const NetDev &N, in
 
 // Steps k .. k+nsteps-1 of the block's neurons (spike list as in k_update_narrow).
 // Populations whose synapses cannot deliver twice in one step take the staged
-// window; the others run step by step.  Three blocks per SM (85 registers).
+// window; the others run step by step.  At most 72 registers a thread: three
+// blocks per SM leave room for one thread-per-neuron block of 256 at 40.
 template <int KIND, int INTEG, int MON, int EN>
-__global__ void __launch_bounds__(kWideThreads, 3) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
+__global__ void __maxnreg__(72) k_update_wide(PopDev P, NetDev N, int rel, int nsteps,
                                                                  double push_inv_dt) {
     __shared__ WideSmem S;
     extern __shared__ __align__(32) unsigned char stage_raw[];
